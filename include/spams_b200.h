@@ -1,0 +1,167 @@
+/* spams_b200.h - C ABI of the B200 batched sparse-coding engine.
+ *
+ * The engine codes every column x_i of a signal matrix X (m x n, column-major)
+ * against a dictionary D (m x K, column-major, unit-norm columns for OMP) with
+ * Orthogonal Matching Pursuit or LARS-Lasso, on one GPU, and returns the codes
+ * as a K x n CSC matrix with row indices sorted inside each column.
+ *
+ * These entry points are what the SPAMS facade calls would bind to; each one
+ * names the reference interface it replaces.  Semantics (argument meaning,
+ * clamps of L, stopping rules, first-index tie-breaks, error strings) follow
+ * the reference; numThreads is accepted and ignored (the work runs on the GPU).
+ *
+ * Host vs device pointers:
+ *   sc_omp_* / sc_lasso_* / sc_lasso_gram_* take HOST arrays and return a CSC
+ *   matrix in malloc'd host arrays (free with sc_csc_free).  They copy the
+ *   inputs to the device, run, and copy the result back (blocking).
+ *   sc_*_dev variants take DEVICE arrays, write the CSC into caller-provided
+ *   device arrays and run asynchronously on the given CUDA stream.
+ *
+ * Every entry point returns an sc_status; sc_last_error() gives a message.
+ * There is no CPU fallback: without a usable CUDA device the calls return
+ * SC_ERR_NO_DEVICE.
+ */
+#ifndef SPAMS_B200_H
+#define SPAMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SC_OK = 0,
+  SC_ERR_INVALID_ARG = 1,    /* null pointer / negative size / bad option */
+  SC_ERR_DIMENSIONS = 2,     /* "incompatible matrix dimensions" (facade throw) */
+  SC_ERR_NO_CRITERION = 3,   /* omp: "You should either provide L, eps or lambda" */
+  SC_ERR_CUDA = 4,           /* a CUDA runtime call failed */
+  SC_ERR_OUT_OF_MEMORY = 5,  /* device or host allocation failed */
+  SC_ERR_NO_DEVICE = 6,      /* no CUDA device / driver: no CPU fallback exists */
+  SC_ERR_CAPACITY = 7,       /* device CSC output arrays too small (nnz reported) */
+  SC_ERR_TIMEOUT = 8,        /* a bounded device-side wait gave up */
+  SC_ERR_UNSUPPORTED = 9     /* option combination not implemented */
+} sc_status;
+
+/* Lasso constraint modes: enum constraint_type, decomp/decomp.h:95. */
+enum { SC_L1COEFFS = 0, SC_L2ERROR = 1, SC_PENALTY = 2 };
+
+/* Numerical form of the correlation / Gram products.
+ *   SC_PREC_FP32: plain FP32 products (CUDA cores), FP32 iterations.
+ *   SC_PREC_BF16X3: tcgen05 tensor-core products from a BF16 hi/lo split
+ *                   (hi*hi + hi*lo + lo*hi, FP32 accumulate), FP32 iterations,
+ *                   FP64 refinement of the final active-set coefficients.
+ * Double-precision entry points always compute in FP64. */
+enum { SC_PREC_FP32 = 0, SC_PREC_BF16X3 = 1 };
+
+/* CSC result in host memory (reference SpMatrix<T>, linalg/linalg.h:775-935):
+ * colptr has n+1 entries (pB; pE = pB+1), rows/vals have nnz entries. */
+typedef struct {
+  int64_t m, n, nnz;
+  int64_t* colptr;
+  int32_t* rows;
+  float* vals;
+} sc_csc_f32;
+
+typedef struct {
+  int64_t m, n, nnz;
+  int64_t* colptr;
+  int32_t* rows;
+  double* vals;
+} sc_csc_f64;
+
+/* Per-call engine options; zero-initialise for defaults. */
+typedef struct {
+  int precision;  /* SC_PREC_* (single precision calls only); default FP32 */
+  int device;     /* CUDA device ordinal; default 0 */
+  int reserved[6];
+} sc_options;
+
+/* ---- library / status ------------------------------------------------- */
+const char* sc_version(void);
+const char* sc_last_error(void);          /* thread-local message of the last failure */
+sc_status sc_device_count(int* count);    /* number of usable CUDA devices */
+void sc_csc_free_f32(sc_csc_f32* a);      /* frees colptr/rows/vals, zeroes the struct */
+void sc_csc_free_f64(sc_csc_f64* a);
+/* Releases the engine's cached device workspaces and streams on all devices. */
+void sc_release_all(void);
+
+/* ---- OMP ----------------------------------------------------------------
+ * Replaces _omp<T> (cpp_library/spams.h:250-293) -> omp<T>
+ * (decomp/decomp.h:322-404) -> coreORMP (decomp/decomp.h:538-640).
+ *   L, eps, lambda: arrays of 1 (scalar) or n (per signal) entries; an array
+ *   with count 0 means "not given" (defaults L=min(m,K), eps=0, lambda=0; at
+ *   least one must be given).  path (optional): K x min(m,K) column-major,
+ *   receives the regularisation path of the first signal. */
+sc_status sc_omp_f32(const float* X, int m, int64_t n, const float* D, int K,
+                     const int* L, int64_t nL, const float* eps, int64_t nEps,
+                     const float* lambda, int64_t nLambda, int numThreads,
+                     float* path, const sc_options* opt, sc_csc_f32* out);
+sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K,
+                     const int* L, int64_t nL, const double* eps, int64_t nEps,
+                     const double* lambda, int64_t nLambda, int numThreads,
+                     double* path, const sc_options* opt, sc_csc_f64* out);
+
+/* ---- LARS-Lasso ---------------------------------------------------------
+ * Replaces _lassoD<T> (cpp_library/spams.h:107-143) -> lasso2<T>
+ * (decomp/decomp.h:1563-1571, 1574-1646) -> coreLARS2 (:1706-1915).
+ *   L < 0: K; max_length_path < 0: 4L; clamps as the facade.
+ *   mode: SC_L1COEFFS / SC_L2ERROR / SC_PENALTY; pos: non-negative codes.
+ *   path (optional): K x max_length_path, path of the first signal.
+ *   ols / cholesky select the reference's Cholesky variant (lasso<T>,
+ *   decomp/decomp.h:735-841); not implemented -> SC_ERR_UNSUPPORTED. */
+sc_status sc_lasso_f32(const float* X, int m, int64_t n, const float* D, int K,
+                       int L, float lambda1, float lambda2, int mode, int pos,
+                       int ols, int numThreads, int max_length_path,
+                       int cholesky, float* path, const sc_options* opt,
+                       sc_csc_f32* out);
+sc_status sc_lasso_f64(const double* X, int m, int64_t n, const double* D, int K,
+                       int L, double lambda1, double lambda2, int mode, int pos,
+                       int ols, int numThreads, int max_length_path,
+                       int cholesky, double* path, const sc_options* opt,
+                       sc_csc_f64* out);
+
+/* Precomputed products: replaces _lassoQq<T> (cpp_library/spams.h:145-188)
+ * -> lasso2<T>(Data X, G, DtX) (decomp/decomp.h:1574-1646).
+ *   Q = G (K x K, used as given: no ridge added), q = D^T X (K x n);
+ *   X only supplies ||x_i||^2 and the signal length m.  lambda2 only enters
+ *   the facade's clamp of L, as in the reference. */
+sc_status sc_lasso_gram_f32(const float* X, int m, int64_t n, const float* Q,
+                            int K, const float* q, int L, float lambda1,
+                            float lambda2, int mode, int pos, int numThreads,
+                            int max_length_path, float* path,
+                            const sc_options* opt, sc_csc_f32* out);
+sc_status sc_lasso_gram_f64(const double* X, int m, int64_t n, const double* Q,
+                            int K, const double* q, int L, double lambda1,
+                            double lambda2, int mode, int pos, int numThreads,
+                            int max_length_path, double* path,
+                            const sc_options* opt, sc_csc_f64* out);
+
+/* ---- device-resident variants -------------------------------------------
+ * Same computations with X and D in DEVICE memory.  The facade defaults are
+ * resolved by the caller: scalar L / eps / lambda are passed by value, and
+ * d_L / d_eps / d_lambda (DEVICE arrays of n entries, or NULL) override them
+ * per signal.  The CSC goes to caller-provided device arrays: d_colptr (n+1
+ * int64), d_rows / d_vals with capacity `cap` entries (n * L_clamped always
+ * fits).  The call enqueues its work on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream); *nnz_out (host) is written after a stream
+ * synchronisation when nnz_out is non-NULL, otherwise the call returns as
+ * soon as the work is enqueued. */
+sc_status sc_omp_f32_dev(const float* dX, int m, int64_t n, const float* dD,
+                         int K, int L, float eps, float lambda, const int* d_L,
+                         const float* d_eps, const float* d_lambda,
+                         int64_t* d_colptr, int32_t* d_rows, float* d_vals,
+                         int64_t cap, int64_t* nnz_out, void* stream,
+                         const sc_options* opt);
+sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD,
+                           int K, int L, float lambda1, float lambda2, int mode,
+                           int pos, int max_length_path, int64_t* d_colptr,
+                           int32_t* d_rows, float* d_vals, int64_t cap,
+                           int64_t* nnz_out, void* stream,
+                           const sc_options* opt);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* SPAMS_B200_H */

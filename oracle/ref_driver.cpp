@@ -1,0 +1,177 @@
+// Test infrastructure only: a C-ABI shim around the SPAMS reference's own
+// C++ facade, compiled straight from the reference's header sources by
+// oracle/build_ref.sh into oracle/_ref/libspams_ref.so.  It is the ground
+// truth the CPU restatement (oracle/sc_oracle.c) and the CUDA engine are
+// checked against, and the "reference" CPU baseline that bench.py times.
+// Nothing in the shipped engine links or calls it.
+//
+// Entry points forward to the reference facade unchanged:
+//   ref_omp_*    -> _omp<T>     cpp_library/spams.h:250-293
+//                   (-> omp<T> decomp/decomp.h:322-404, coreORMP :538-640)
+//   ref_lasso_*  -> _lassoD<T>  cpp_library/spams.h:107-143
+//                   (-> lasso2<T> decomp/decomp.h:1563-1646, coreLARS2 :1706-1915,
+//                    or lasso<T>/coreLARS when cholesky/ols is set)
+//   ref_lassoQq_* -> _lassoQq<T> cpp_library/spams.h:145-188
+// Outputs are copied out of the reference's SpMatrix<T> (linalg/linalg.h:775-935)
+// into malloc'd CSC arrays released by ref_free().
+#include "cppspams.h"
+#include <cstdlib>
+#include <cstring>
+#include <cstdint>
+
+extern "C" {
+
+typedef struct {
+  int64_t m, n, nnz;
+  int64_t* colptr;  // n+1
+  int32_t* rows;    // nnz
+  void* vals;       // nnz of T
+  char err[128];    // facade exception text, "" on success
+} ref_csc;
+
+void ref_free(void* p) { free(p); }
+
+}  // extern "C"
+
+template <typename T>
+static void copy_out(SpMatrix<T>* a, ref_csc* out) {
+  const int64_t n = a->n();
+  out->m = a->m();
+  out->n = n;
+  const int64_t nnz = n > 0 ? a->pB()[n] : 0;
+  out->nnz = nnz;
+  out->colptr = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  out->rows = (int32_t*)malloc(sizeof(int32_t) * (nnz > 0 ? nnz : 1));
+  out->vals = malloc(sizeof(T) * (nnz > 0 ? nnz : 1));
+  for (int64_t i = 0; i <= n; ++i) out->colptr[i] = n > 0 ? a->pB()[i] : 0;
+  for (int64_t i = 0; i < nnz; ++i) {
+    out->rows[i] = a->r()[i];
+    ((T*)out->vals)[i] = a->v()[i];
+  }
+}
+
+template <typename T>
+static int run_omp(const T* X, int m, int n, const T* D, int K, const int* L,
+                   int nL, const T* eps, int nEps, const T* lambda, int nLambda,
+                   int numThreads, T* path, ref_csc* out) {
+  memset(out, 0, sizeof(*out));
+  Matrix<T> mX(const_cast<T*>(X), m, n);
+  Matrix<T> mD(const_cast<T*>(D), m, K);
+  int Ldummy = 0;
+  T edummy = 0, ldummy = 0;
+  Vector<int> vL(nL > 0 ? const_cast<int*>(L) : &Ldummy, nL > 0 ? nL : 1);
+  Vector<T> vE(nEps > 0 ? const_cast<T*>(eps) : &edummy, nEps > 0 ? nEps : 1);
+  Vector<T> vLa(nLambda > 0 ? const_cast<T*>(lambda) : &ldummy,
+                nLambda > 0 ? nLambda : 1);
+  Matrix<T>* p = NULL;
+  SpMatrix<T>* a = NULL;
+  try {
+    a = _omp<T>(&mX, &mD, &p, path != NULL, nL > 0, &vL, nEps > 0, &vE,
+                nLambda > 0, &vLa, numThreads);
+  } catch (const char* e) {
+    strncpy(out->err, e, sizeof(out->err) - 1);
+    return 1;
+  }
+  copy_out(a, out);
+  if (path && p) memcpy(path, p->rawX(), sizeof(T) * p->m() * p->n());
+  delete a;
+  delete p;
+  return 0;
+}
+
+template <typename T>
+static int run_lasso(const T* X, int m, int n, const T* D, int K, int L,
+                     T lambda1, T lambda2, int mode, int pos, int ols,
+                     int cholesky, int numThreads, int max_length_path, T* path,
+                     ref_csc* out) {
+  memset(out, 0, sizeof(*out));
+  Matrix<T> mX(const_cast<T*>(X), m, n);
+  Matrix<T> mD(const_cast<T*>(D), m, K);
+  Matrix<T>* p = NULL;
+  SpMatrix<T>* a = NULL;
+  try {
+    a = _lassoD<T>(&mX, &mD, &p, path != NULL, L, lambda1, lambda2,
+                   (constraint_type)mode, pos != 0, ols != 0, numThreads,
+                   max_length_path, false, cholesky != 0);
+  } catch (const char* e) {
+    strncpy(out->err, e, sizeof(out->err) - 1);
+    return 1;
+  }
+  copy_out(a, out);
+  if (path && p) memcpy(path, p->rawX(), sizeof(T) * p->m() * p->n());
+  delete a;
+  delete p;
+  return 0;
+}
+
+template <typename T>
+static int run_lassoQq(const T* X, int m, int n, const T* Q, int K, const T* q,
+                       int L, T lambda1, int mode, int pos, int numThreads,
+                       int max_length_path, T* path, ref_csc* out) {
+  memset(out, 0, sizeof(*out));
+  Matrix<T> mX(const_cast<T*>(X), m, n);
+  Matrix<T> mQ(const_cast<T*>(Q), K, K);
+  Matrix<T> mq(const_cast<T*>(q), K, n);
+  Matrix<T>* p = NULL;
+  SpMatrix<T>* a = NULL;
+  try {
+    a = _lassoQq<T>(&mX, &mQ, &mq, &p, path != NULL, L, lambda1, T(0),
+                    (constraint_type)mode, pos != 0, false, numThreads,
+                    max_length_path, false, false);
+  } catch (const char* e) {
+    strncpy(out->err, e, sizeof(out->err) - 1);
+    return 1;
+  }
+  copy_out(a, out);
+  if (path && p) memcpy(path, p->rawX(), sizeof(T) * p->m() * p->n());
+  delete a;
+  delete p;
+  return 0;
+}
+
+extern "C" {
+
+int ref_omp_f64(const double* X, int m, int n, const double* D, int K,
+                const int* L, int nL, const double* eps, int nEps,
+                const double* lambda, int nLambda, int numThreads, double* path,
+                ref_csc* out) {
+  return run_omp<double>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda,
+                         numThreads, path, out);
+}
+int ref_omp_f32(const float* X, int m, int n, const float* D, int K,
+                const int* L, int nL, const float* eps, int nEps,
+                const float* lambda, int nLambda, int numThreads, float* path,
+                ref_csc* out) {
+  return run_omp<float>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda,
+                        numThreads, path, out);
+}
+int ref_lasso_f64(const double* X, int m, int n, const double* D, int K, int L,
+                  double lambda1, double lambda2, int mode, int pos, int ols,
+                  int cholesky, int numThreads, int max_length_path,
+                  double* path, ref_csc* out) {
+  return run_lasso<double>(X, m, n, D, K, L, lambda1, lambda2, mode, pos, ols,
+                           cholesky, numThreads, max_length_path, path, out);
+}
+int ref_lasso_f32(const float* X, int m, int n, const float* D, int K, int L,
+                  float lambda1, float lambda2, int mode, int pos, int ols,
+                  int cholesky, int numThreads, int max_length_path,
+                  float* path, ref_csc* out) {
+  return run_lasso<float>(X, m, n, D, K, L, lambda1, lambda2, mode, pos, ols,
+                          cholesky, numThreads, max_length_path, path, out);
+}
+int ref_lassoQq_f64(const double* X, int m, int n, const double* Q, int K,
+                    const double* q, int L, double lambda1, int mode, int pos,
+                    int numThreads, int max_length_path, double* path,
+                    ref_csc* out) {
+  return run_lassoQq<double>(X, m, n, Q, K, q, L, lambda1, mode, pos,
+                             numThreads, max_length_path, path, out);
+}
+int ref_lassoQq_f32(const float* X, int m, int n, const float* Q, int K,
+                    const float* q, int L, float lambda1, int mode, int pos,
+                    int numThreads, int max_length_path, float* path,
+                    ref_csc* out) {
+  return run_lassoQq<float>(X, m, n, Q, K, q, L, lambda1, mode, pos,
+                            numThreads, max_length_path, path, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,392 @@
+/* Test infrastructure only (the oracle): a plain-C restatement of the SPAMS
+ * reference's OMP and LARS-Lasso coding path, used by tests/ and by bench.py's
+ * CPU-baseline leg as the checker.  The shipped engine never links it.
+ *
+ * This file is included twice by sc_oracle.c, once with T=double/SUF=f64 and
+ * once with T=float/SUF=f32, so every routine exists in both precisions like
+ * the reference's templates.  Loops replace the reference's BLAS calls, so
+ * low-order bits can differ from a BLAS build (summation order); the control
+ * flow, stopping rules and tie-breaks are the reference's.
+ */
+#define CAT2(a, b) a##_##b
+#define CAT(a, b) CAT2(a, b)
+#define F(name) CAT(name, SUF)
+/* MIN macro of linalg/utils.h:46 (a NaN first argument is kept). */
+#define ORC_MIN(a, b) (((a) > (b)) ? (b) : (a))
+
+/* cblas_iamax semantics (linalg/cblas_alt_template.h:787-797 -> BLAS i?amax):
+ * first index of the largest magnitude. */
+static int F(orc_iamax)(int n, const T* x) {
+  int best = 0;
+  T bv = n > 0 ? (T)fabs((double)x[0]) : 0;
+  for (int j = 1; j < n; ++j) {
+    T v = (T)fabs((double)x[j]);
+    if (v > bv) { bv = v; best = j; }
+  }
+  return best;
+}
+
+/* Vector<T>::max (linalg/linalg.h:2769-2780): first index of the largest value. */
+static int F(orc_argmax)(int n, const T* x) {
+  int best = 0;
+  T bv = x[0];
+  for (int j = 1; j < n; ++j)
+    if (x[j] > bv) { bv = x[j]; best = j; }
+  return best;
+}
+
+/* The reference's own cblas_iamin (linalg/cblas_alt_template.h:1094-1105):
+ * first index of the smallest magnitude, comparisons in double. */
+static int F(orc_iamin)(int n, const T* x) {
+  int imin = 0;
+  double mn = fabs((double)x[0]);
+  for (int j = 1; j < n; ++j) {
+    double cur = fabs((double)x[j]);
+    if (cur < mn) { imin = j; mn = cur; }
+  }
+  return imin;
+}
+
+/* x[0:n] <- U[0:n,0:n] x, U upper triangular, column-major with leading
+ * dimension ld (BLAS trmv Upper/NoTrans/NonUnit). */
+static void F(orc_trmv_upper)(int n, const T* U, int ld, T* x) {
+  for (int r = 0; r < n; ++r) {
+    T s = 0;
+    for (int k = r; k < n; ++k) s += U[r + (size_t)k * ld] * x[k];
+    x[r] = s;
+  }
+}
+
+/* y = A x for symmetric A of order n stored in its upper triangle
+ * (BLAS symv Upper). */
+static void F(orc_symv_upper)(int n, const T* A, int ld, const T* x, T* y) {
+  for (int r = 0; r < n; ++r) {
+    T s = 0;
+    for (int c = 0; c < n; ++c) {
+      const T a = r <= c ? A[r + (size_t)c * ld] : A[c + (size_t)r * ld];
+      s += a * x[c];
+    }
+    y[r] = s;
+  }
+}
+
+/* A += alpha x x^T on the upper triangle (BLAS syr Upper). */
+static void F(orc_syr_upper)(int n, T alpha, const T* x, T* A, int ld) {
+  for (int c = 0; c < n; ++c) {
+    const T t = alpha * x[c];
+    for (int r = 0; r <= c; ++r) A[r + (size_t)c * ld] += t * x[r];
+  }
+}
+
+/* G = D^T D (+ ridge on the diagonal): Matrix::XtX (linalg/linalg.h:1967-1972)
+ * followed by ProdMatrix::addDiag when ridge != 0. */
+void F(orc_gram)(const T* D, int m, int K, T ridge, T* G) {
+  for (int a = 0; a < K; ++a)
+    for (int b = a; b < K; ++b) {
+      T s = 0;
+      for (int r = 0; r < m; ++r) s += D[r + (size_t)a * m] * D[r + (size_t)b * m];
+      G[a + (size_t)b * K] = s;
+      G[b + (size_t)a * K] = s;
+    }
+  if (ridge != 0)
+    for (int a = 0; a < K; ++a) G[a + (size_t)a * K] += ridge;
+}
+
+/* y = D^T x (Matrix::multTrans, linalg/linalg.h:1751-1756). */
+static void F(orc_dtx)(const T* D, int m, int K, const T* x, T* y) {
+  for (int k = 0; k < K; ++k) {
+    T s = 0;
+    for (int r = 0; r < m; ++r) s += D[r + (size_t)k * m] * x[r];
+    y[k] = s;
+  }
+}
+
+/* coreORMP (decomp/decomp.h:538-640) for one signal.
+ *   Rdn:  D^T x on entry (overwritten with the residual correlations)
+ *   Lcap: the driver's clamped L (Gs.n() in the reference); L: this signal's L
+ *   ind:  Lcap entries, -1 terminated on return; RUn: Lcap coefficients
+ *   path: K x Lcap or NULL
+ * Returns the number of selected atoms. */
+int F(orc_omp_signal)(const T* G, int K, T* Rdn, T normX, int Lcap, int Lsig,
+                      T eps_in, T lambda, int* ind, T* RUn, T* path) {
+  const T eps = (T)fabs((double)eps_in);
+  const int L = Lsig < Lcap ? Lsig : Lcap;
+  for (int j = 0; j < Lcap; ++j) { ind[j] = -1; RUn[j] = 0; }
+  /* L < 0 reaches undefined behaviour in the reference (negative memset
+   * when a path is requested); it selects nothing otherwise. */
+  if (normX <= eps || L <= 0) return 0;
+  T* scores = (T*)malloc(sizeof(T) * K);
+  T* norm = (T*)malloc(sizeof(T) * K);
+  T* Un = (T*)calloc((size_t)L * L, sizeof(T));
+  T* Undn = (T*)calloc((size_t)K * L, sizeof(T));
+  for (int k = 0; k < K; ++k) { scores[k] = Rdn[k]; norm[k] = 1; }
+  if (path) memset(path, 0, sizeof(T) * (size_t)K * L);
+  int j;
+  for (j = 0; j < L; ++j) {
+    const int c = F(orc_iamax)(K, scores);
+    if (norm[c] < 1e-8) { ind[j] = -1; break; }
+    const T invNorm = (T)1.0 / (T)sqrt((double)norm[c]);
+    const T RU = Rdn[c] * invNorm;
+    const T delta = RU * RU;
+    if (delta < 2 * lambda) break;
+    RUn[j] = RU;
+    normX -= delta;
+    ind[j] = c;
+    /* new inverse-Cholesky column: Un[:,j] = invNorm [ -Un_j Undn[c,0:j] ; 1 ] */
+    T* col = Un + (size_t)j * L;
+    col[j] = -1;
+    for (int k = 0; k < j; ++k) col[k] = Undn[c + (size_t)k * K];
+    F(orc_trmv_upper)(j, Un, L, col);
+    for (int k = 0; k <= j; ++k) col[k] *= -invNorm;
+    if (j == L - 1 || normX <= eps) { ++j; break; }
+    if (path) {
+      T* last = path + (size_t)(L - 1) * K;
+      for (int k = 0; k <= j; ++k) last[k] = RUn[k];
+      F(orc_trmv_upper)(j + 1, Un, L, last);
+      for (int k = 0; k <= j; ++k) path[(size_t)j * K + ind[k]] = last[k];
+    }
+    /* Undn[:,j] = G[:, ind[0:j+1]] Un[0:j+1, j] */
+    T* und = Undn + (size_t)j * K;
+    for (int r = 0; r < K; ++r) {
+      T s = 0;
+      for (int k = 0; k <= j; ++k) s += G[r + (size_t)ind[k] * K] * col[k];
+      und[r] = s;
+    }
+    for (int r = 0; r < K; ++r) {
+      Rdn[r] += und[r] * (-RUn[j]);
+      norm[r] -= und[r] * und[r];
+      scores[r] = (Rdn[r] * Rdn[r]) / norm[r];
+    }
+    for (int k = 0; k <= j; ++k) scores[ind[k]] = 0;
+  }
+  F(orc_trmv_upper)(j, Un, L, RUn);
+  if (path) {
+    memset(path + (size_t)(L - 1) * K, 0, sizeof(T) * L);
+    for (int k = 0; k < j; ++k) path[(size_t)(j - 1) * K + ind[k]] = RUn[k];
+  }
+  free(scores); free(norm); free(Un); free(Undn);
+  return j;
+}
+
+/* coreLARS2 (decomp/decomp.h:1706-1915) for one signal.
+ *   DtR: D^T x on entry (overwritten);  G includes the ridge.
+ *   LL:  the driver's L;  coeffs/ind: LL entries.
+ *   path: K x length_path or NULL.  Returns the number of active atoms. */
+int F(orc_lars_signal)(const T* G, int K, T* DtR, T normX, int LL, int mode,
+                       T constraint, int pos, int length_path, int* ind,
+                       T* coeffs, T* path) {
+  const int L = LL < K ? LL : K;
+  if (length_path <= 1) length_path = 4 * L;
+  for (int j = 0; j < LL; ++j) { coeffs[j] = 0; ind[j] = -1; }
+  if (L <= 0) return 0;
+  int cur = pos ? F(orc_argmax)(K, DtR) : F(orc_iamax)(K, DtR);
+  if (mode == 2 && fabs((double)DtR[cur]) < constraint) return 0;
+  if (mode == 1 && normX < constraint) return 0;
+  T* Gs = (T*)calloc((size_t)LL * LL, sizeof(T));
+  T* invGs = (T*)calloc((size_t)LL * LL, sizeof(T));
+  T* Ga = (T*)calloc((size_t)K * LL, sizeof(T));
+  T* work = (T*)calloc((size_t)K * 3, sizeof(T));
+  T* u = (T*)calloc((size_t)K, sizeof(T));
+  const T INF = (T)INFINITY;
+  int newAtom = 1, i, iter = 0;
+  T thrs = 0;
+  for (i = 0; i < L; ++i) {
+    ++iter;
+    if (newAtom) {
+      ind[i] = cur;
+      memcpy(Ga + (size_t)i * K, G + (size_t)cur * K, sizeof(T) * K);
+      for (int j = 0; j <= i; ++j) Gs[(size_t)i * LL + j] = Ga[(size_t)i * K + ind[j]];
+      if (i == 0) {
+        invGs[0] = (T)1.0 / Gs[0];
+      } else {
+        F(orc_symv_upper)(i, invGs, LL, Gs + (size_t)i * LL, u);
+        T d = 0;
+        for (int j = 0; j < i; ++j) d += u[j] * Gs[(size_t)i * LL + j];
+        const T schur = (T)1.0 / (Gs[(size_t)i * LL + i] - d);
+        invGs[(size_t)i * LL + i] = schur;
+        for (int j = 0; j < i; ++j) invGs[(size_t)i * LL + j] = -schur * u[j];
+        F(orc_syr_upper)(i, schur, u, invGs, LL);
+      }
+    }
+    for (int j = 0; j <= i; ++j) work[j] = DtR[ind[j]] > 0 ? (T)1.0 : (T)-1.0;
+    F(orc_symv_upper)(i + 1, invGs, LL, work, u);
+    T step_max = INF;
+    int first_zero = -1;
+    for (int j = 0; j <= i; ++j) {
+      const T ratio = -coeffs[j] / u[j];
+      if (ratio > 0 && ratio <= step_max) { step_max = ratio; first_zero = j; }
+    }
+    const T C = (T)fabs((double)DtR[ind[0]]);
+    T* A = work + 2 * (size_t)K;
+    for (int r = 0; r < K; ++r) {
+      T s = 0;
+      for (int j = 0; j <= i; ++j) s += Ga[r + (size_t)j * K] * u[j];
+      A[r] = s;
+    }
+    for (int r = 0; r < K; ++r) { work[r] = A[r]; work[r + K] = A[r]; }
+    for (int j = 0; j <= i; ++j) { work[ind[j]] = INF; work[ind[j] + K] = INF; }
+    for (int r = 0; r < K; ++r)
+      work[r] = (work[r] < INF && work[r] > (T)-1.0) ? (DtR[r] + C) / ((T)1.0 + work[r]) : INF;
+    for (int r = 0; r < K; ++r)
+      work[r + K] = (work[r + K] < INF && work[r + K] < (T)1.0) ? (C - DtR[r]) / ((T)1.0 - work[r + K]) : INF;
+    if (pos)
+      for (int r = 0; r < K; ++r) work[r] = INF;
+    const int index = F(orc_iamin)(2 * K, work);
+    T step = work[index];
+    cur = index % K;
+    T coeff1 = 0, coeff2 = 0;
+    for (int j = 0; j <= i; ++j) coeff1 += DtR[ind[j]] > 0 ? u[j] : -u[j];
+    for (int j = 0; j <= i; ++j) coeff2 += DtR[ind[j]] * u[j];
+    const T coeff3 = normX - constraint;
+    T step_max2;
+    if (mode == 2) {
+      step_max2 = C - constraint;
+    } else if (mode == 1) {
+      const T delta = coeff2 * coeff2 - coeff1 * coeff3;
+      step_max2 = delta < 0 ? INF : (coeff2 - (T)sqrt((double)delta)) / coeff1;
+      step_max2 = ORC_MIN(C, step_max2);
+    } else {
+      step_max2 = coeff1 < 0 ? INF : (constraint - thrs) / coeff1;
+      step_max2 = ORC_MIN(C, step_max2);
+    }
+    step = ORC_MIN(ORC_MIN(step, step_max2), step_max);
+    if (step == INF) break;
+    for (int j = 0; j <= i; ++j) coeffs[j] += step * u[j];
+    if (pos)
+      for (int j = 0; j <= i; ++j) if (coeffs[j] < 0) coeffs[j] = 0;
+    for (int r = 0; r < K; ++r) DtR[r] += (-step) * A[r];
+    normX += coeff1 * step * step - 2 * coeff2 * step;
+    thrs += step * coeff1;
+    if (path)
+      for (int k = 0; k <= i; ++k) path[(size_t)iter * K + ind[k]] = coeffs[k];
+    if (step == step_max) {
+      const int fz = first_zero;
+      for (int j = fz; j < i; ++j) {
+        memcpy(Ga + (size_t)j * K, Ga + (size_t)(j + 1) * K, sizeof(T) * K);
+        ind[j] = ind[j + 1];
+        coeffs[j] = coeffs[j + 1];
+      }
+      ind[i] = -1;
+      coeffs[i] = 0;
+      for (int j = fz; j < i; ++j) {
+        memmove(Gs + (size_t)j * LL, Gs + (size_t)(j + 1) * LL, sizeof(T) * fz);
+        memmove(Gs + (size_t)j * LL + fz, Gs + (size_t)(j + 1) * LL + fz + 1, sizeof(T) * (i - fz));
+      }
+      const T schur = invGs[(size_t)fz * LL + fz];
+      for (int j = 0; j < fz; ++j) u[j] = invGs[(size_t)fz * LL + j];
+      for (int j = fz; j < i; ++j) u[j] = invGs[(size_t)(j + 1) * LL + fz];
+      for (int j = fz; j < i; ++j) {
+        memmove(invGs + (size_t)j * LL, invGs + (size_t)(j + 1) * LL, sizeof(T) * fz);
+        memmove(invGs + (size_t)j * LL + fz, invGs + (size_t)(j + 1) * LL + fz + 1, sizeof(T) * (i - fz));
+      }
+      F(orc_syr_upper)(i, (T)-1.0 / schur, u, invGs, LL);
+      newAtom = 0;
+      i = i - 2;
+    } else {
+      newAtom = 1;
+    }
+    if ((iter >= length_path - 1) || fabs((double)step) < 1e-15 || step == step_max2 ||
+        (normX < 1e-15) || (i == (L - 1)) ||
+        (mode == 1 && normX - constraint < 1e-15) ||
+        (mode == 0 && (constraint - thrs < 1e-15)))
+      break;
+  }
+  free(Gs); free(invGs); free(Ga); free(work); free(u);
+  int cnt = 0;
+  while (cnt < LL && ind[cnt] >= 0) ++cnt;
+  return cnt;
+}
+
+/* SpMatrix::convert (linalg/linalg.h:4840-4861): dense L x n (value, row)
+ * pairs, -1 terminated per column, to CSC with rows sorted ascending
+ * (misc.h:137-166 quicksort; any correct sort gives the same result since
+ * rows are distinct).  colptr has n+1 entries. */
+int64_t F(orc_convert)(const T* vM, const int* rM, int L, int64_t n,
+                       int64_t* colptr, int* rows, T* vals) {
+  int64_t cnt = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    colptr[i] = cnt;
+    const int64_t beg = cnt;
+    for (int j = 0; j < L; ++j) {
+      const int r = rM[(size_t)i * L + j];
+      if (r == -1) break;
+      if (rows) {
+        /* insertion into the sorted run [beg, cnt) */
+        int64_t p = cnt;
+        while (p > beg && rows[p - 1] > r) { rows[p] = rows[p - 1]; vals[p] = vals[p - 1]; --p; }
+        rows[p] = r;
+        vals[p] = vM[(size_t)i * L + j];
+      }
+      ++cnt;
+    }
+  }
+  colptr[n] = cnt;
+  return cnt;
+}
+
+/* omp<T> driver (decomp/decomp.h:322-404) with the _omp facade's defaults
+ * (cpp_library/spams.h:250-293) already resolved by the caller:
+ *   Lv/nL: scalar (nL == 1) or per-column L; likewise eps and lambda.
+ * Writes vM (Lc x n) and rM (Lc x n) where Lc = the clamped L (returned). */
+int F(orc_omp)(const T* X, int m, int64_t n, const T* D, int K, const int* Lv,
+               int nL, const T* eps, int nEps, const T* lambda, int nLambda,
+               T* vM, int* rM, T* path, int Lc_cap) {
+  int L = Lv[0];
+  if (nL > 1)
+    for (int64_t i = 1; i < n; ++i) if (Lv[i] > L) L = Lv[i];
+  if (L <= 0) return 0;
+  if (L > K) L = K;
+  if (L > m) L = m;
+  if (Lc_cap > 0 && L > Lc_cap) return -1;
+  T* G = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* Rdn = (T*)malloc(sizeof(T) * (size_t)K);
+  F(orc_gram)(D, m, K, 0, G);
+  for (int64_t i = 0; i < n; ++i) {
+    const T* x = X + (size_t)i * m;
+    T normX = 0;
+    for (int r = 0; r < m; ++r) normX += x[r] * x[r];
+    F(orc_dtx)(D, m, K, x, Rdn);
+    F(orc_omp_signal)(G, K, Rdn, normX, L, nL > 1 ? Lv[i] : Lv[0],
+                      nEps > 1 ? eps[i] : eps[0], nLambda > 1 ? lambda[i] : lambda[0],
+                      rM + (size_t)i * L, vM + (size_t)i * L, (path && i == 0) ? path : NULL);
+  }
+  free(G); free(Rdn);
+  return L;
+}
+
+/* Facade clamps of _lassoD (cpp_library/spams.h:107-130): returns the L that
+ * lasso2 receives and writes the path length through *max_length_path. */
+int F(orc_lasso_clamp)(int m, int K, int L, T lambda1, T lambda2, int mode,
+                       int pos, int* max_length_path) {
+  if (L < 0) L = K;
+  if (*max_length_path < 0) *max_length_path = 4 * L;
+  if (L > m && !(mode == 2 && fabs((double)lambda1) < 1e-99 && !pos && lambda2 > 0)) L = m;
+  if (L > K) L = K;
+  return L;
+}
+
+/* lasso2<T>(X, D, ...) driver (decomp/decomp.h:1563-1646), L already clamped:
+ * G = D^T D + max(lambda2, 1e-10) I, per-column D^T x, coreLARS2. */
+void F(orc_lasso)(const T* X, int m, int64_t n, const T* D, int K, int L,
+                  T lambda1, T lambda2, int mode, int pos, int length_path,
+                  T* vM, int* rM, T* path) {
+  if (L <= 0) return;
+  T* G = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* DtR = (T*)malloc(sizeof(T) * (size_t)K);
+  const T ridge = lambda2 > (T)1e-10 ? lambda2 : (T)1e-10;
+  F(orc_gram)(D, m, K, ridge, G);
+  for (int64_t i = 0; i < n; ++i) {
+    const T* x = X + (size_t)i * m;
+    T normX = 0;
+    for (int r = 0; r < m; ++r) normX += x[r] * x[r];
+    F(orc_dtx)(D, m, K, x, DtR);
+    F(orc_lars_signal)(G, K, DtR, normX, L, mode, lambda1, pos, length_path,
+                       rM + (size_t)i * L, vM + (size_t)i * L, (path && i == 0) ? path : NULL);
+  }
+  free(G); free(DtR);
+}
+
+#undef F
+#undef ORC_MIN
+#undef CAT
+#undef CAT2

@@ -1,0 +1,719 @@
+// Host engine behind the C ABI (include/spams_b200.h): argument checks and
+// the reference facade's clamps, per-device workspaces and streams, and the
+// chunked coding pipeline
+//     ||x||^2, D^T X  ->  per-signal OMP / LARS  ->  overflow rerun  ->  CSC
+// All arithmetic runs on the GPU; there is no CPU fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/spams_b200.h"
+#include "engine.h"
+#include "kernels.h"
+
+namespace sc {
+
+// ---------------------------------------------------------------------------
+// errors
+static thread_local char g_err[512] = "";
+
+sc_status fail(sc_status st, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return st;
+}
+const char* last_error() { return g_err; }
+
+#define SC_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t _e = (call);                                                       \
+    if (_e != cudaSuccess)                                                         \
+      return fail(_e == cudaErrorMemoryAllocation ? SC_ERR_OUT_OF_MEMORY          \
+                                                  : SC_ERR_CUDA,                   \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
+                  __LINE__);                                                       \
+  } while (0)
+
+#define SC_TRY(expr)                    \
+  do {                                  \
+    sc_status _s = (expr);              \
+    if (_s != SC_OK) return _s;         \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers (grow-only, cached per device)
+sc_status Buf::reserve(size_t b) {
+  if (b <= bytes) return SC_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  const size_t want = std::max(b, (size_t)256);
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    cudaGetLastError();
+    return fail(SC_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu bytes) failed: %s", want,
+                cudaGetErrorString(e));
+  }
+  bytes = want;
+  return SC_OK;
+}
+void Buf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+static std::mutex g_ctx_mu;
+static std::vector<DeviceCtx*> g_ctx;
+
+sc_status get_ctx(int device, DeviceCtx** out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return fail(SC_ERR_NO_DEVICE, "no CUDA device available (%s); the engine has no CPU path",
+                e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+  }
+  if (device < 0 || device >= count)
+    return fail(SC_ERR_INVALID_ARG, "device %d out of range (%d devices)", device, count);
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if ((int)g_ctx.size() < count) g_ctx.resize(count, nullptr);
+  SC_CUDA(cudaSetDevice(device));
+  if (!g_ctx[device]) {
+    DeviceCtx* c = new DeviceCtx();
+    c->device = device;
+    SC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    SC_CUDA(cudaEventCreateWithFlags(&c->last_use, cudaEventDisableTiming));
+    SC_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    SC_CUDA(cudaHostAlloc(&c->pinned_small, 4096, cudaHostAllocDefault));
+    g_ctx[device] = c;
+  }
+  *out = g_ctx[device];
+  return SC_OK;
+}
+
+void release_all() {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  for (DeviceCtx*& c : g_ctx) {
+    if (!c) continue;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (Buf* b : c->all_bufs()) b->release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->last_use) cudaEventDestroy(c->last_use);
+    if (c->pinned_small) cudaFreeHost(c->pinned_small);
+    delete c;
+    c = nullptr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch shapes
+struct Shape {
+  int Lcap;   // active-set capacity in shared memory
+  int wpb;    // warps per block
+  int grid;   // persistent blocks
+};
+
+template <typename T>
+static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
+  Shape s;
+  s.Lcap = std::max(1, std::min(L, 32));
+  s.wpb = 8;
+  const size_t per_warp = lars ? lars_state_bytes(Kp, s.Lcap, sizeof(T))
+                               : omp_state_bytes(Kp, s.Lcap, sizeof(T));
+  while (s.wpb > 1 && (size_t)s.wpb * per_warp > (size_t)c.smem_per_block) s.wpb >>= 1;
+  const size_t per_block = (size_t)s.wpb * per_warp + 1024;
+  int bps = (int)((size_t)c.smem_per_sm / per_block);
+  const int regw = lars ? lars_max_warps_per_sm<T>(Kp) : omp_max_warps_per_sm<T>(Kp);
+  bps = std::min(bps, std::max(1, regw / s.wpb));
+  bps = std::max(1, std::min(bps, 64 / s.wpb));
+  s.grid = c.num_sms * bps;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// the coding pipeline
+template <typename T>
+struct Problem {
+  bool lars = true;
+  const T* dX = nullptr;          // device X (m x n)
+  const T* hX = nullptr;          // host X, staged chunk by chunk
+  const T* dDtX = nullptr;        // device D^T X given by the caller (K x n)
+  const T* dD = nullptr;          // device D (m x K)
+  int m = 0;
+  int64_t n = 0;
+  int K = 0, Kp = 0;
+  int L = 0;                      // clamped driver L (slab stride)
+  int mode = 2; T lambda1 = 0; int pos = 0; int length_path = 0;
+  int Lsig = 0; T eps = 0, lambda = 0;
+  const int* dLv = nullptr; const T* dEps = nullptr; const T* dLam = nullptr;
+  // device CSC output (device entry points); unused with a host sink
+  int64_t* d_colptr = nullptr; int32_t* d_rows = nullptr; T* d_vals = nullptr;
+  int64_t cap = 0;
+  T* d_path = nullptr;            // device path of signal 0 (zeroed), or nullptr
+};
+
+template <typename T>
+struct HostSink {
+  std::vector<int64_t> colptr;
+  std::vector<int32_t> rows;
+  std::vector<T> vals;
+};
+
+template <typename T>
+static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
+                              HostSink<T>* sink, int* d_capflag) {
+  const int Kp = p.Kp;
+  const Shape shp = pick_shape<T>(c, p.lars, Kp, p.L);
+  // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
+  const size_t per_sig = (size_t)Kp * sizeof(T) + (size_t)p.L * (sizeof(T) + 4) + 64 +
+                         (p.hX ? (size_t)p.m * sizeof(T) : 0) +
+                         (sink ? (size_t)p.L * (sizeof(T) + 4) + 8 : 0);
+  int64_t nc = (int64_t)std::max<size_t>(4096, ((size_t)2 << 30) / per_sig);
+  nc = std::min<int64_t>(nc, std::max<int64_t>(p.n, 1));
+  nc = std::min<int64_t>(nc, (int64_t)1 << 30);
+
+  SC_TRY(c.dtx.reserve((size_t)Kp * nc * sizeof(T)));
+  SC_TRY(c.norms.reserve((size_t)nc * sizeof(T)));
+  SC_TRY(c.slab_ind.reserve((size_t)nc * p.L * 4));
+  SC_TRY(c.slab_val.reserve((size_t)nc * p.L * sizeof(T)));
+  SC_TRY(c.cnt.reserve((size_t)nc * 4));
+  SC_TRY(c.ovf_list.reserve((size_t)nc * 8));
+  SC_TRY(c.misc.reserve(256));
+  const int64_t scan_len = scan_scratch_len(nc);
+  SC_TRY(c.scan.reserve((size_t)scan_len * 8));
+  if (p.hX) SC_TRY(c.xstage.reserve((size_t)nc * p.m * sizeof(T)));
+  if (sink) {
+    SC_TRY(c.ccolptr.reserve((size_t)(nc + 1) * 8));
+    SC_TRY(c.crows.reserve((size_t)nc * p.L * 4));
+    SC_TRY(c.cvals.reserve((size_t)nc * p.L * sizeof(T)));
+    sink->colptr.assign((size_t)p.n + 1, 0);
+  }
+  // overflow pass: state in global slabs with capacity L
+  const int ovf_wpb = 4;
+  const size_t ovf_per_warp = p.lars ? lars_state_bytes(Kp, p.L, sizeof(T))
+                                     : omp_state_bytes(Kp, p.L, sizeof(T));
+  int ovf_grid = c.num_sms;
+  while (ovf_grid > 1 && (size_t)ovf_grid * ovf_wpb * ovf_per_warp > ((size_t)256 << 20))
+    ovf_grid >>= 1;
+  const bool may_overflow = shp.Lcap < p.L;
+  if (may_overflow) SC_TRY(c.gstate.reserve((size_t)ovf_grid * ovf_wpb * ovf_per_warp));
+
+  unsigned* d_counter = reinterpret_cast<unsigned*>(c.misc.ptr);   // [0], [1]
+  int* d_ovf_count = reinterpret_cast<int*>(c.misc.ptr) + 4;         // [4]
+
+  int64_t nnz_total = 0;
+  for (int64_t start = 0; start < p.n; start += nc) {
+    const int64_t cn = std::min<int64_t>(nc, p.n - start);
+    T* dtx = reinterpret_cast<T*>(c.dtx.ptr);
+    T* norms = reinterpret_cast<T*>(c.norms.ptr);
+    // ---- inputs: ||x||^2 and D^T x
+    const T* xchunk = nullptr;
+    if (p.hX) {
+      SC_CUDA(cudaMemcpyAsync(c.xstage.ptr, p.hX + (size_t)start * p.m,
+                              (size_t)cn * p.m * sizeof(T), cudaMemcpyHostToDevice, st));
+      xchunk = reinterpret_cast<const T*>(c.xstage.ptr);
+    } else {
+      xchunk = p.dX + (size_t)start * p.m;
+    }
+    SC_CUDA(launch_colnorms<T>(xchunk, p.m, cn, norms, st));
+    if (p.dDtX)
+      SC_CUDA(launch_pad_rows<T>(p.dDtX + (size_t)start * p.K, p.K, p.K, cn, dtx, Kp, st));
+    else
+      SC_CUDA(launch_gemm_tn<T>(p.dD, p.m, p.K, xchunk, p.m, cn, p.m, dtx, Kp, Kp, st));
+    // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
+    SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
+    int* cnt = reinterpret_cast<int*>(c.cnt.ptr);
+    int* sind = reinterpret_cast<int*>(c.slab_ind.ptr);
+    T* sval = reinterpret_cast<T*>(c.slab_val.ptr);
+    int64_t* ovf_list = reinterpret_cast<int64_t*>(c.ovf_list.ptr);
+    T* path = start == 0 ? p.d_path : nullptr;
+    if (p.lars) {
+      LarsArgs<T> a{};
+      a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
+      a.Lcap = shp.Lcap; a.mode = p.mode; a.constraint = p.lambda1; a.pos = p.pos;
+      a.length_path = p.length_path; a.n_jobs = (int)cn; a.n_jobs_dev = nullptr;
+      a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
+      a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
+      a.gstate = nullptr; a.path = path;
+      SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
+      if (may_overflow) {
+        a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
+        a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
+        a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+        SC_CUDA(launch_lars<T>(a, ovf_grid, ovf_wpb, st));
+      }
+    } else {
+      OmpArgs<T> a{};
+      a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
+      a.Lcap = shp.Lcap; a.eps = p.eps; a.lambda = p.lambda; a.Lsig = p.Lsig;
+      a.vL = p.dLv ? p.dLv + start : nullptr;
+      a.vEps = p.dEps ? p.dEps + start : nullptr;
+      a.vLambda = p.dLam ? p.dLam + start : nullptr;
+      a.n_jobs = (int)cn; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
+      a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
+      a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
+      a.path = path;
+      SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
+      if (may_overflow) {
+        a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
+        a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
+        a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+        SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
+      }
+    }
+    // ---- CSC
+    int64_t* scratch = reinterpret_cast<int64_t*>(c.scan.ptr);
+    if (sink) {
+      int64_t* ccol = reinterpret_cast<int64_t*>(c.ccolptr.ptr);
+      SC_CUDA(launch_scan_counts(cnt, cn, ccol, nullptr, scratch, scan_len, st));
+      SC_CUDA(launch_csc_gather<T>(sind, sval, p.L, cnt, ccol, cn, nullptr, cn * (int64_t)p.L,
+                                   d_capflag, reinterpret_cast<int32_t*>(c.crows.ptr),
+                                   reinterpret_cast<T*>(c.cvals.ptr), st));
+      std::vector<int64_t> hcol((size_t)cn + 1);
+      SC_CUDA(cudaMemcpyAsync(hcol.data(), ccol, (size_t)(cn + 1) * 8, cudaMemcpyDeviceToHost, st));
+      SC_CUDA(cudaStreamSynchronize(st));
+      const int64_t cnnz = hcol[cn];
+      const size_t old = sink->rows.size();
+      sink->rows.resize(old + cnnz);
+      sink->vals.resize(old + cnnz);
+      if (cnnz > 0) {
+        SC_CUDA(cudaMemcpyAsync(sink->rows.data() + old, c.crows.ptr, (size_t)cnnz * 4,
+                                cudaMemcpyDeviceToHost, st));
+        SC_CUDA(cudaMemcpyAsync(sink->vals.data() + old, c.cvals.ptr, (size_t)cnnz * sizeof(T),
+                                cudaMemcpyDeviceToHost, st));
+      }
+      for (int64_t i = 0; i <= cn; ++i) sink->colptr[start + i] = nnz_total + hcol[i];
+      nnz_total += cnnz;
+      SC_CUDA(cudaStreamSynchronize(st));
+    } else {
+      int64_t* col = p.d_colptr + start;
+      SC_CUDA(launch_scan_counts(cnt, cn, col, start == 0 ? nullptr : col, scratch, scan_len, st));
+      SC_CUDA(launch_csc_gather<T>(sind, sval, p.L, cnt, col, cn, nullptr, p.cap, d_capflag,
+                                   p.d_rows, p.d_vals, st));
+    }
+  }
+  return SC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// result helpers
+template <typename T> struct CscOf;
+template <> struct CscOf<float> { using type = sc_csc_f32; };
+template <> struct CscOf<double> { using type = sc_csc_f64; };
+
+template <typename T>
+static sc_status emit_empty(int64_t m, int64_t n, typename CscOf<T>::type* out) {
+  out->m = m;
+  out->n = n;
+  out->nnz = 0;
+  out->colptr = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+  out->rows = (int32_t*)malloc(sizeof(int32_t));
+  out->vals = (T*)malloc(sizeof(T));
+  if (!out->colptr || !out->rows || !out->vals) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+  return SC_OK;
+}
+
+template <typename T>
+static sc_status emit_sink(int64_t m, int64_t n, HostSink<T>& s, typename CscOf<T>::type* out) {
+  out->m = m;
+  out->n = n;
+  out->nnz = s.colptr.empty() ? 0 : s.colptr.back();
+  out->colptr = (int64_t*)malloc(sizeof(int64_t) * ((size_t)n + 1));
+  out->rows = (int32_t*)malloc(sizeof(int32_t) * std::max<size_t>(1, s.rows.size()));
+  out->vals = (T*)malloc(sizeof(T) * std::max<size_t>(1, s.vals.size()));
+  if (!out->colptr || !out->rows || !out->vals) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+  if (n >= 0) memcpy(out->colptr, s.colptr.data(), sizeof(int64_t) * ((size_t)n + 1));
+  if (!s.rows.empty()) memcpy(out->rows, s.rows.data(), sizeof(int32_t) * s.rows.size());
+  if (!s.vals.empty()) memcpy(out->vals, s.vals.data(), sizeof(T) * s.vals.size());
+  return SC_OK;
+}
+
+static inline int pad128(int K) { return ((K + 127) / 128) * 128; }
+
+// Per-call device guard: serialises calls on one device and orders this
+// call's stream after the previous user of the shared workspaces.
+struct CallGuard {
+  DeviceCtx* c;
+  cudaStream_t st;
+  std::lock_guard<std::mutex> lk;
+  CallGuard(DeviceCtx* ctx, cudaStream_t s) : c(ctx), st(s), lk(ctx->mu) {
+    cudaStreamWaitEvent(st, c->last_use, 0);
+  }
+  ~CallGuard() { cudaEventRecord(c->last_use, st); }
+};
+
+static sc_status check_kp(int K) {
+  if (pad128(K) > 1024)
+    return fail(SC_ERR_UNSUPPORTED, "dictionaries with more than 1024 atoms are not supported yet (K=%d)", K);
+  return SC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// OMP (host arrays)
+template <typename T>
+static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const int* Lv,
+                          int64_t nL, const T* eps, int64_t nEps, const T* lam, int64_t nLam,
+                          T* path, const sc_options* opt, typename CscOf<T>::type* out) {
+  if (!out) return fail(SC_ERR_INVALID_ARG, "omp : null output");
+  memset(out, 0, sizeof(*out));
+  if (m < 0 || n < 0 || K < 0) return fail(SC_ERR_INVALID_ARG, "omp : negative dimension");
+  if ((n > 0 && m > 0 && !X) || (K > 0 && m > 0 && !D))
+    return fail(SC_ERR_INVALID_ARG, "omp : null input matrix");
+  if (nL == 0 && nEps == 0 && nLam == 0)
+    return fail(SC_ERR_NO_CRITERION, "omp : You should either provide L, eps or lambda");
+  auto bad_count = [&](int64_t c) { return c < 0 || (c > 1 && c != n); };
+  if (bad_count(nL) || bad_count(nEps) || bad_count(nLam))
+    return fail(SC_ERR_INVALID_ARG, "omp : L/eps/lambda must hold 1 or n entries");
+  if ((nL > 0 && !Lv) || (nEps > 0 && !eps) || (nLam > 0 && !lam))
+    return fail(SC_ERR_INVALID_ARG, "omp : null L/eps/lambda array");
+  const int scalar_L = std::min(m, K);
+  const bool vecL = nL > 1, vecE = nEps > 1, vecLa = nLam > 1;
+  const int Lsig = nL == 0 ? scalar_L : Lv[0];
+  const T eps0 = nEps == 0 ? T(0) : eps[0];
+  const T lam0 = nLam == 0 ? T(0) : lam[0];
+  if (path) memset(path, 0, sizeof(T) * (size_t)K * scalar_L);
+  int L = Lsig;
+  if (vecL) {
+    L = Lv[0];
+    for (int64_t i = 1; i < n; ++i) L = std::max(L, Lv[i]);
+  }
+  if (L <= 0) return emit_empty<T>(0, 0, out);  // spalpha.clear(); return
+  L = std::min(m, std::min(L, K));
+  if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
+  SC_TRY(check_kp(K));
+
+  DeviceCtx* c = nullptr;
+  SC_TRY(get_ctx(opt ? opt->device : 0, &c));
+  CallGuard g(c, c->stream);
+  cudaStream_t st = c->stream;
+  const int Kp = pad128(K);
+  SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
+  SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
+  SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
+  SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, T(0), (T*)c->G.ptr, st));
+  // per-signal vectors
+  const size_t vbytes = (vecL ? 4 * (size_t)n : 0) + (vecE ? sizeof(T) * (size_t)n : 0) +
+                        (vecLa ? sizeof(T) * (size_t)n : 0) + 64;
+  SC_TRY(c->vecs.reserve(vbytes));
+  char* vp = (char*)c->vecs.ptr;
+  Problem<T> p;
+  p.lars = false;
+  if (vecE) {
+    p.dEps = (const T*)vp;
+    SC_CUDA(cudaMemcpyAsync(vp, eps, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+    vp += align16(sizeof(T) * n);
+  }
+  if (vecLa) {
+    p.dLam = (const T*)vp;
+    SC_CUDA(cudaMemcpyAsync(vp, lam, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+    vp += align16(sizeof(T) * n);
+  }
+  if (vecL) {
+    p.dLv = (const int*)vp;
+    SC_CUDA(cudaMemcpyAsync(vp, Lv, 4 * (size_t)n, cudaMemcpyHostToDevice, st));
+  }
+  p.hX = X; p.dD = (const T*)c->D.ptr; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
+  p.Lsig = Lsig; p.eps = eps0; p.lambda = lam0;
+  if (path) {
+    SC_TRY(c->path.reserve(sizeof(T) * (size_t)K * scalar_L));
+    SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * scalar_L, st));
+    p.d_path = (T*)c->path.ptr;
+  }
+  SC_TRY(c->misc.reserve(256));
+  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  HostSink<T> sink;
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag));
+  if (path)
+    SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * scalar_L,
+                            cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaStreamSynchronize(st));
+  return emit_sink<T>(K, n, sink, out);
+}
+
+// ---------------------------------------------------------------------------
+// LARS-Lasso (host arrays)
+template <typename T>
+static int lasso_clamp(int m, int K, int L, T lambda1, T lambda2, int mode, int pos,
+                       int* max_length_path) {
+  // _lassoD / _lassoQq, cpp_library/spams.h:116-130
+  if (L < 0) L = K;
+  if (*max_length_path < 0) *max_length_path = 4 * L;
+  const bool keep = mode == SC_PENALTY && std::fabs((double)lambda1) < 1e-99 && !pos && lambda2 > 0;
+  if (L > m && !keep) L = m;
+  if (L > K) L = K;
+  return L;
+}
+
+template <typename T>
+static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q, const T* q,
+                            int K, int L, T lambda1, T lambda2, int mode, int pos, int ols,
+                            int max_length_path, int cholesky, T* path, const sc_options* opt,
+                            typename CscOf<T>::type* out) {
+  if (!out) return fail(SC_ERR_INVALID_ARG, "lasso : null output");
+  memset(out, 0, sizeof(*out));
+  if (m < 0 || n < 0 || K < 0) return fail(SC_ERR_INVALID_ARG, "lasso : negative dimension");
+  if (n > 0 && m > 0 && !X) return fail(SC_ERR_INVALID_ARG, "lasso : null X");
+  if (Q) {
+    if (K > 0 && !Q) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
+    if (K > 0 && n > 0 && !q) return fail(SC_ERR_INVALID_ARG, "lasso : null q");
+  } else if (K > 0 && m > 0 && !D) {
+    return fail(SC_ERR_INVALID_ARG, "lasso : null D");
+  }
+  if (mode < 0 || mode > 2)
+    return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d not supported by the coding path", mode);
+  L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
+  if (ols || cholesky)
+    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky/ols variant (lasso<T>, coreLARS) is not implemented");
+  if (path) memset(path, 0, sizeof(T) * (size_t)K * std::max(0, max_length_path));
+  if (L <= 0) return emit_empty<T>(0, 0, out);
+  if (n == 0) return emit_empty<T>(K, 0, out);
+  SC_TRY(check_kp(K));
+
+  DeviceCtx* c = nullptr;
+  SC_TRY(get_ctx(opt ? opt->device : 0, &c));
+  CallGuard g(c, c->stream);
+  cudaStream_t st = c->stream;
+  const int Kp = pad128(K);
+  SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
+  Problem<T> p;
+  p.lars = true;
+  if (Q) {
+    // use Q as given (no ridge), zero padded
+    SC_TRY(c->D.reserve((size_t)K * K * sizeof(T) + (size_t)K * n * sizeof(T)));
+    SC_CUDA(cudaMemcpyAsync(c->D.ptr, Q, (size_t)K * K * sizeof(T), cudaMemcpyHostToDevice, st));
+    SC_CUDA(launch_pad_rows<T>((const T*)c->D.ptr, K, K, K, (T*)c->G.ptr, Kp, st));
+    if (Kp > K)
+      SC_CUDA(cudaMemsetAsync((T*)c->G.ptr + (size_t)Kp * K, 0, sizeof(T) * (size_t)Kp * (Kp - K), st));
+    T* dq = (T*)c->D.ptr + (size_t)K * K;
+    SC_CUDA(cudaMemcpyAsync(dq, q, (size_t)K * n * sizeof(T), cudaMemcpyHostToDevice, st));
+    p.dDtX = dq;
+  } else {
+    SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
+    SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
+    const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);  // MAX(lambda2, 1e-10)
+    SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, ridge, (T*)c->G.ptr, st));
+    p.dD = (const T*)c->D.ptr;
+  }
+  p.hX = X; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
+  p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
+  if (path && max_length_path > 0) {
+    SC_TRY(c->path.reserve(sizeof(T) * (size_t)K * max_length_path));
+    SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * max_length_path, st));
+    p.d_path = (T*)c->path.ptr;
+  }
+  SC_TRY(c->misc.reserve(256));
+  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  HostSink<T> sink;
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag));
+  if (p.d_path)
+    SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * max_length_path,
+                            cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaStreamSynchronize(st));
+  return emit_sink<T>(K, n, sink, out);
+}
+
+// ---------------------------------------------------------------------------
+// device-resident entry points
+template <typename T>
+static sc_status finish_dev(DeviceCtx* c, cudaStream_t st, int64_t* d_colptr, int64_t n,
+                            int* d_capflag, int64_t* nnz_out) {
+  if (!nnz_out) return SC_OK;
+  int64_t* h = reinterpret_cast<int64_t*>(c->pinned_small);
+  SC_CUDA(cudaMemcpyAsync(h, d_colptr + n, 8, cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaMemcpyAsync(h + 1, d_capflag, 4, cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaStreamSynchronize(st));
+  *nnz_out = h[0];
+  if (*reinterpret_cast<int*>(h + 1))
+    return fail(SC_ERR_CAPACITY, "output capacity too small: nnz = %lld",
+                (long long)h[0]);
+  return SC_OK;
+}
+
+template <typename T>
+static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, int L, T lambda1,
+                           T lambda2, int mode, int pos, int max_length_path,
+                           int64_t* d_colptr, int32_t* d_rows, T* d_vals, int64_t cap,
+                           int64_t* nnz_out, void* stream, const sc_options* opt) {
+  if (m <= 0 || n < 0 || K <= 0) return fail(SC_ERR_INVALID_ARG, "lasso : bad dimensions");
+  if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
+    return fail(SC_ERR_INVALID_ARG, "lasso : null device pointer");
+  if (mode < 0 || mode > 2) return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d", mode);
+  L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
+  SC_TRY(check_kp(K));
+  DeviceCtx* c = nullptr;
+  SC_TRY(get_ctx(opt ? opt->device : 0, &c));
+  cudaStream_t st = (cudaStream_t)stream;
+  CallGuard g(c, st);
+  SC_TRY(c->misc.reserve(256));
+  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
+  if (n == 0 || L <= 0) {
+    SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
+    return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
+  }
+  const int Kp = pad128(K);
+  SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
+  const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
+  SC_CUDA(launch_gram<T>(dD, m, K, Kp, ridge, (T*)c->G.ptr, st));
+  Problem<T> p;
+  p.lars = true; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
+  p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
+  p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag));
+  return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
+}
+
+template <typename T>
+static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int Lsig, T eps,
+                         T lambda, const int* d_L, const T* d_eps, const T* d_lambda,
+                         int64_t* d_colptr, int32_t* d_rows, T* d_vals, int64_t cap,
+                         int64_t* nnz_out, void* stream, const sc_options* opt) {
+  if (m <= 0 || n < 0 || K <= 0) return fail(SC_ERR_INVALID_ARG, "omp : bad dimensions");
+  if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
+    return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
+  SC_TRY(check_kp(K));
+  DeviceCtx* c = nullptr;
+  SC_TRY(get_ctx(opt ? opt->device : 0, &c));
+  cudaStream_t st = (cudaStream_t)stream;
+  CallGuard g(c, st);
+  SC_TRY(c->misc.reserve(256));
+  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
+  // the driver L: with per-signal L the caller passes their maximum as Lsig
+  int L = std::min(m, std::min(Lsig, K));
+  if (n == 0 || L <= 0) {
+    SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
+    return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
+  }
+  const int Kp = pad128(K);
+  SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
+  SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));
+  Problem<T> p;
+  p.lars = false; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
+  p.Lsig = Lsig; p.eps = eps; p.lambda = lambda; p.dLv = d_L; p.dEps = d_eps; p.dLam = d_lambda;
+  p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag));
+  return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
+}
+
+}  // namespace sc
+
+// ---------------------------------------------------------------------------
+// C ABI
+using namespace sc;
+
+extern "C" {
+
+const char* sc_version(void) { return "spams_b200 0.1"; }
+const char* sc_last_error(void) { return sc::last_error(); }
+
+sc_status sc_device_count(int* count) {
+  if (!count) return fail(SC_ERR_INVALID_ARG, "null count");
+  *count = 0;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return fail(SC_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+  }
+  return SC_OK;
+}
+
+void sc_csc_free_f32(sc_csc_f32* a) {
+  if (!a) return;
+  free(a->colptr); free(a->rows); free(a->vals);
+  memset(a, 0, sizeof(*a));
+}
+void sc_csc_free_f64(sc_csc_f64* a) {
+  if (!a) return;
+  free(a->colptr); free(a->rows); free(a->vals);
+  memset(a, 0, sizeof(*a));
+}
+void sc_release_all(void) { sc::release_all(); }
+
+sc_status sc_omp_f32(const float* X, int m, int64_t n, const float* D, int K, const int* L,
+                     int64_t nL, const float* eps, int64_t nEps, const float* lambda,
+                     int64_t nLambda, int numThreads, float* path, const sc_options* opt,
+                     sc_csc_f32* out) {
+  (void)numThreads;
+  return omp_host<float>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out);
+}
+sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K, const int* L,
+                     int64_t nL, const double* eps, int64_t nEps, const double* lambda,
+                     int64_t nLambda, int numThreads, double* path, const sc_options* opt,
+                     sc_csc_f64* out) {
+  (void)numThreads;
+  return omp_host<double>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out);
+}
+
+sc_status sc_lasso_f32(const float* X, int m, int64_t n, const float* D, int K, int L,
+                       float lambda1, float lambda2, int mode, int pos, int ols, int numThreads,
+                       int max_length_path, int cholesky, float* path, const sc_options* opt,
+                       sc_csc_f32* out) {
+  (void)numThreads;
+  return lasso_host<float>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos, ols,
+                           max_length_path, cholesky, path, opt, out);
+}
+sc_status sc_lasso_f64(const double* X, int m, int64_t n, const double* D, int K, int L,
+                       double lambda1, double lambda2, int mode, int pos, int ols,
+                       int numThreads, int max_length_path, int cholesky, double* path,
+                       const sc_options* opt, sc_csc_f64* out) {
+  (void)numThreads;
+  return lasso_host<double>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos,
+                            ols, max_length_path, cholesky, path, opt, out);
+}
+
+sc_status sc_lasso_gram_f32(const float* X, int m, int64_t n, const float* Q, int K,
+                            const float* q, int L, float lambda1, float lambda2, int mode,
+                            int pos, int numThreads, int max_length_path, float* path,
+                            const sc_options* opt, sc_csc_f32* out) {
+  (void)numThreads;
+  if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
+  static const float dummy = 0;
+  return lasso_host<float>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
+                           pos, 0, max_length_path, 0, path, opt, out);
+}
+sc_status sc_lasso_gram_f64(const double* X, int m, int64_t n, const double* Q, int K,
+                            const double* q, int L, double lambda1, double lambda2, int mode,
+                            int pos, int numThreads, int max_length_path, double* path,
+                            const sc_options* opt, sc_csc_f64* out) {
+  (void)numThreads;
+  if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
+  static const double dummy = 0;
+  return lasso_host<double>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
+                            pos, 0, max_length_path, 0, path, opt, out);
+}
+
+sc_status sc_omp_f32_dev(const float* dX, int m, int64_t n, const float* dD, int K, int L,
+                         float eps, float lambda, const int* d_L, const float* d_eps,
+                         const float* d_lambda, int64_t* d_colptr, int32_t* d_rows,
+                         float* d_vals, int64_t cap, int64_t* nnz_out, void* stream,
+                         const sc_options* opt) {
+  return omp_dev<float>(dX, m, n, dD, K, L, eps, lambda, d_L, d_eps, d_lambda, d_colptr, d_rows,
+                        d_vals, cap, nnz_out, stream, opt);
+}
+
+sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD, int K, int L,
+                           float lambda1, float lambda2, int mode, int pos, int max_length_path,
+                           int64_t* d_colptr, int32_t* d_rows, float* d_vals, int64_t cap,
+                           int64_t* nnz_out, void* stream, const sc_options* opt) {
+  return lasso_dev<float>(dX, m, n, dD, K, L, lambda1, lambda2, mode, pos, max_length_path,
+                          d_colptr, d_rows, d_vals, cap, nnz_out, stream, opt);
+}
+
+}  // extern "C"

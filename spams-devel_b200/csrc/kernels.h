@@ -1,0 +1,125 @@
+// Kernel argument blocks and launch entry points shared by the engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace sc {
+
+// Leading dimension of the small per-signal square matrices (inverse Gram,
+// inverse Cholesky factor): odd, so that lanes walking a column hit distinct
+// shared-memory banks.
+__host__ __device__ inline int state_ld(int Lc) { return (Lc & 1) ? Lc : Lc + 1; }
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+// Per-warp LARS state: DtR[Kp], invGs[Lc x ld], u/coef/sign/cA/w/g[Lc], ind[Lc].
+__host__ __device__ inline size_t lars_state_bytes(int Kp, int Lc, size_t esz) {
+  return align16(esz * ((size_t)Kp + (size_t)Lc * state_ld(Lc) + 6 * (size_t)Lc) +
+                 4 * (size_t)Lc);
+}
+
+// Per-warp OMP state: Rdn[Kp], norm[Kp], Un[Lc x ld], RUn/vec/g[Lc], ind[Lc].
+__host__ __device__ inline size_t omp_state_bytes(int Kp, int Lc, size_t esz) {
+  return align16(esz * (2 * (size_t)Kp + (size_t)Lc * state_ld(Lc) + 3 * (size_t)Lc) +
+                 4 * (size_t)Lc);
+}
+
+template <typename T>
+struct LarsArgs {
+  const T* G;          // Kp x Kp, ld Kp, ridge included, zero padded
+  const T* DtX;        // Kp x n, ld Kp (zero rows beyond K)
+  const T* norms;      // n: ||x_i||^2
+  int K, Kp;           // atoms, padded to a multiple of 128
+  int L;               // driver L (clamped by the facade): slab stride, path cap
+  int Lcap;            // active-set capacity of the per-warp state
+  int mode;            // 0 L1COEFFS, 1 L2ERROR, 2 PENALTY
+  T constraint;        // lambda1
+  int pos;
+  int length_path;
+  int n_jobs;          // signals in this launch
+  const int* n_jobs_dev;    // if set, the job count is read from device memory
+  const int64_t* sig_list;  // job -> signal index, or NULL for identity
+  unsigned* work_counter;   // queue head, zero at launch
+  int* out_ind;        // n x L slabs: sorted atom indices
+  T* out_val;          // n x L slabs: coefficients
+  int* out_cnt;        // n: active-set size (0 for overflowed signals)
+  int64_t* overflow_list;   // signals whose active set outgrew Lcap
+  int* overflow_count;
+  T* gstate;           // NULL: state in shared memory; else per-warp global slabs
+  T* path;             // K x length_path for signal 0, or NULL
+};
+
+template <typename T>
+struct OmpArgs {
+  const T* G;          // Kp x Kp, ld Kp, no ridge, zero padded
+  const T* DtX;        // Kp x n
+  const T* norms;      // n
+  int K, Kp;
+  int L;               // driver L: min(m, L, K); slab stride
+  int Lcap;
+  T eps, lambda;       // scalar stopping values
+  int Lsig;            // scalar per-signal L (before the min with L)
+  const int* vL;       // per-signal L (device) or NULL
+  const T* vEps;       // per-signal eps or NULL
+  const T* vLambda;    // per-signal lambda or NULL
+  int n_jobs;
+  const int* n_jobs_dev;
+  const int64_t* sig_list;
+  unsigned* work_counter;
+  int* out_ind;
+  T* out_val;
+  int* out_cnt;
+  int64_t* overflow_list;
+  int* overflow_count;
+  T* gstate;
+  T* path;             // K x L for signal 0, or NULL
+};
+
+template <typename T>
+cudaError_t launch_lars(const LarsArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);
+template <typename T>
+int lars_max_warps_per_sm(int Kp);
+
+template <typename T>
+cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);
+template <typename T>
+int omp_max_warps_per_sm(int Kp);
+
+// ---- dense products ------------------------------------------------------
+// C (Kp x n, ld ldc) = A^T B with A m x Ka (ld lda), B m x n (ld ldb),
+// column-major; rows Ka..Kp-1 of C are written as zero.
+template <typename T>
+cudaError_t launch_gemm_tn(const T* A, int lda, int Ka, const T* B, int ldb,
+                           int64_t n, int m, T* C, int ldc, int Kp, cudaStream_t st);
+// G (Kp x Kp) = D^T D + ridge I on the first K diagonal entries, symmetric,
+// zero beyond K.
+template <typename T>
+cudaError_t launch_gram(const T* D, int m, int K, int Kp, T ridge, T* G, cudaStream_t st);
+// norms[i] = ||x_i||^2
+template <typename T>
+cudaError_t launch_colnorms(const T* X, int m, int64_t n, T* norms, cudaStream_t st);
+// Copy a K x n block (ld ldsrc) into a Kp x n block (ld Kp), zero padding.
+template <typename T>
+cudaError_t launch_pad_rows(const T* src, int K, int64_t ldsrc, int64_t n, T* dst,
+                            int Kp, cudaStream_t st);
+
+// ---- CSC assembly ----------------------------------------------------------
+// colptr[i+1] = base + cnt[0] + ... + cnt[i]; with base == NULL the base is 0
+// and colptr[0] is written as 0, otherwise colptr[0] is left alone (it is
+// *base, written by the previous chunk).
+cudaError_t launch_scan_counts(const int* cnt, int64_t n, int64_t* colptr, const int64_t* base,
+                               int64_t* scratch, int64_t scratch_len, cudaStream_t st);
+int64_t scan_scratch_len(int64_t n);
+// rows/vals[colptr[i] - *sub + j] = slab pairs of column i (sub NULL: 0).
+// A column that would not fit in `cap` entries is skipped and *capflag set.
+template <typename T>
+cudaError_t launch_csc_gather(const int* slab_ind, const T* slab_val, int L,
+                              const int* cnt, const int64_t* colptr, int64_t n,
+                              const int64_t* sub, int64_t cap, int* capflag,
+                              int32_t* rows, T* vals, cudaStream_t st);
+
+// ---- BF16 hi/lo split tensor-core products (sm_100a tcgen05) --------------
+bool tc_gemm_available();
+
+}  // namespace sc

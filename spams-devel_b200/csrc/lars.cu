@@ -1,0 +1,405 @@
+// LARS-Lasso homotopy for every signal of a batch: one warp per signal,
+// persistent grid fed by a device work counter.
+//
+// Restates coreLARS2 (decomp/decomp.h:1706-1915) step for step:
+//   - add atom: inverse-Gram Schur update of invGs (symv / dot / syr, :1749-1771)
+//   - direction u = invGs sign(DtR_A) (:1774-1777)
+//   - zero-crossing step, last index among equal ratios ("<=", :1780-1788)
+//   - A = Ga u over the active Gram columns (:1792-1795)
+//   - joining steps over inactive atoms, first minimum of the 2K magnitudes
+//     (the reference's own cblas_iamin, linalg/cblas_alt_template.h:1094-1105)
+//   - mode bound step_max2 (:1826-1847), MIN macro of linalg/utils.h:46
+//   - coefficient / correlation / normX / thrs updates (:1848-1866)
+//   - drop + inverse downdate (:1875-1903), stopping rules (:1907-1913)
+//
+// Layout: G is Kp x Kp column-major (ld Kp, ridge on the diagonal, zero rows /
+// columns beyond K); DtX is Kp x n column-major.  Lane `l` of a warp owns the
+// rows r = 128 v + 4 l + e (v < NV, e < 4), so every Gram-column read is one
+// 512-byte coalesced vector load per v.  The per-signal state (correlations,
+// inverse Gram, active set) sits in shared memory, or, for the overflow pass
+// that reruns signals whose active set outgrew the shared-memory capacity, in
+// a global scratch slab per warp.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace sc {
+
+__device__ __forceinline__ int own_lane(int r) { return (r & 127) >> 2; }
+__device__ __forceinline__ int own_bit(int r) { return ((r >> 7) << 2) | (r & 3); }
+
+// MIN macro of linalg/utils.h:46.
+template <typename T> __device__ __forceinline__ T ref_min(T a, T b) { return a > b ? b : a; }
+
+template <typename T, int NV>
+__global__ void __launch_bounds__(256)
+lars_kernel(const LarsArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int Lc = a.Lcap;
+  const int ldi = state_ld(Lc);
+  const size_t per_warp = lars_state_bytes(a.Kp, Lc, sizeof(T));
+  unsigned char* base =
+      a.gstate ? reinterpret_cast<unsigned char*>(a.gstate) +
+                     (size_t)(blockIdx.x * wpb + wib) * per_warp
+               : smem_raw + (size_t)wib * per_warp;
+  T* sDtR = reinterpret_cast<T*>(base);
+  T* sInv = sDtR + a.Kp;
+  T* sU = sInv + (size_t)Lc * ldi;
+  T* sCoef = sU + Lc;
+  T* sS = sCoef + Lc;
+  T* sCA = sS + Lc;
+  T* sW = sCA + Lc;
+  T* sG = sW + Lc;
+  int* sInd = reinterpret_cast<int*>(sG + Lc);
+
+  const int K = a.K, Kp = a.Kp;
+  const T INF = inf<T>();
+  const int L = a.L < K ? a.L : K;  // L = MIN(LL, K)
+  const int length_path = a.length_path <= 1 ? 4 * L : a.length_path;
+  const int mode = a.mode;
+  const T constraint = a.constraint;
+  const bool pos = a.pos != 0;
+
+  const int n_jobs = a.n_jobs_dev ? *a.n_jobs_dev : a.n_jobs;
+  for (;;) {
+    int job = 0;
+    if (lane == 0) job = (int)atomicAdd(a.work_counter, 1u);
+    job = __shfl_sync(kFull, job, 0);
+    if (job >= n_jobs) break;
+    const int64_t sig = a.sig_list ? a.sig_list[job] : (int64_t)job;
+    T* path = (a.path && sig == 0) ? a.path : nullptr;
+
+    // ---- load D^T x and find the first atom
+    const T* dtx = a.DtX + (size_t)sig * Kp;
+    T bkey = -INF;
+    int bidx = 0x7fffffff;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const int r0 = v * 128 + lane * 4;
+      const Vec4<T> d = ldg4(dtx + r0);
+      st4(sDtR + r0, d);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = r0 + e;
+        if (r < K) {
+          const T key = pos ? d.v[e] : fabs(d.v[e]);
+          if (key > bkey || (key == bkey && r < bidx)) { bkey = key; bidx = r; }
+        }
+      }
+    }
+    warp_argmax(bkey, bidx);
+    int cur = bidx;
+    T normX = a.norms[sig];
+    for (int j = lane; j < Lc; j += 32) sCoef[j] = 0;  // coeffs.setZeros()
+    __syncwarp();
+
+    int cnt = 0;
+    bool overflow = false;
+    bool skip = L <= 0;
+    if (!skip) {
+      const T dc = sDtR[cur];
+      if (mode == 2 && fabs(dc) < constraint) skip = true;
+      if (mode == 1 && normX < constraint) skip = true;
+    }
+
+    uint32_t act = 0;  // active flags of this lane's rows
+    if (!skip) {
+      bool newAtom = true;
+      int iter = 0;
+      T thrs = 0;
+      for (int i = 0; i < L; ++i) {
+        ++iter;
+        if (newAtom) {
+          if (i >= Lc) { overflow = true; break; }
+          if (lane == 0) sInd[i] = cur;
+          if (lane == own_lane(cur)) act |= 1u << own_bit(cur);
+          ++cnt;
+          __syncwarp();
+          const T* gcol = a.G + (size_t)cur * Kp;
+          for (int j = lane; j <= i; j += 32) sG[j] = gcol[sInd[j]];
+          __syncwarp();
+          if (i == 0) {
+            if (lane == 0) sInv[0] = T(1) / sG[0];
+          } else {
+            // w = invGs(0:i,0:i) g(0:i)
+            for (int r = lane; r < i; r += 32) {
+              T s = 0;
+              const T* row = sInv + (size_t)r * ldi;
+              for (int c = 0; c < i; ++c) s += row[c] * sG[c];
+              sW[r] = s;
+            }
+            __syncwarp();
+            T part = 0;
+            for (int r = lane; r < i; r += 32) part += sW[r] * sG[r];
+            const T dot = warp_sum(part);
+            const T schur = T(1) / (sG[i] - dot);
+            for (int r = lane; r < i; r += 32) {
+              T* row = sInv + (size_t)r * ldi;
+              const T wr = sW[r];
+              for (int c = 0; c < i; ++c) {
+                const T whi = c > r ? sW[c] : wr;
+                const T wlo = c > r ? wr : sW[c];
+                row[c] += (schur * whi) * wlo;
+              }
+              const T off = (-schur) * wr;
+              row[i] = off;
+              sInv[(size_t)i * ldi + r] = off;
+            }
+            if (lane == 0) sInv[(size_t)i * ldi + i] = schur;
+          }
+          __syncwarp();
+        }
+
+        // ---- direction u = invGs sign(DtR_A)
+        for (int j = lane; j <= i; j += 32) {
+          const T d = sDtR[sInd[j]];
+          sCA[j] = d;
+          sS[j] = d > 0 ? T(1) : T(-1);
+        }
+        __syncwarp();
+        T zkey = INF;
+        int zidx = -1;
+        for (int r = lane; r <= i; r += 32) {
+          T s = 0;
+          const T* row = sInv + (size_t)r * ldi;
+          for (int c = 0; c <= i; ++c) s += row[c] * sS[c];
+          sU[r] = s;
+          const T ratio = -sCoef[r] / s;
+          if (ratio > 0 && ratio <= zkey) { zkey = ratio; zidx = r; }
+        }
+        warp_argmin_last(zkey, zidx);
+        const T step_max = zkey;
+        const int first_zero = zidx;
+        __syncwarp();
+        const T C = fabs(sCA[0]);
+
+        // ---- A = Ga u
+        T A[NV][4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) A[v][e] = 0;
+#pragma unroll 4
+        for (int j = 0; j <= i; ++j) {
+          const T uj = sU[j];
+          const T* gc = a.G + (size_t)sInd[j] * Kp + lane * 4;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            const Vec4<T> g = ldg4(gc + v * 128);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) A[v][e] += g.v[e] * uj;
+          }
+        }
+
+        // ---- joining steps: first minimum magnitude over the 2K candidates
+        T mkey = INF, mval = INF;
+        int midx = 0x7fffffff;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const int r0 = v * 128 + lane * 4;
+          const Vec4<T> d = ld4(sDtR + r0);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int r = r0 + e;
+            if (r < K) {
+              const bool active = (act >> (v * 4 + e)) & 1u;
+              const T aa = A[v][e];
+              T c1 = INF, c2 = INF;
+              if (!active && aa < INF) {
+                if (!pos && aa > T(-1)) c1 = (d.v[e] + C) / (T(1) + aa);
+                if (aa < T(1)) c2 = (C - d.v[e]) / (T(1) - aa);
+              }
+              const T k1 = fabs(c1), k2 = fabs(c2);
+              if (k1 < mkey || (k1 == mkey && r < midx)) { mkey = k1; midx = r; mval = c1; }
+              if (k2 < mkey || (k2 == mkey && r + K < midx)) { mkey = k2; midx = r + K; mval = c2; }
+            }
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const T k2 = __shfl_xor_sync(kFull, mkey, o);
+          const int i2 = __shfl_xor_sync(kFull, midx, o);
+          const T v2 = __shfl_xor_sync(kFull, mval, o);
+          if (k2 < mkey || (k2 == mkey && i2 < midx)) { mkey = k2; midx = i2; mval = v2; }
+        }
+        T step = mval;
+        cur = midx % K;
+
+        // ---- polynomial of normX along the step
+        T p1 = 0, p2 = 0;
+        for (int j = lane; j <= i; j += 32) {
+          const T uj = sU[j];
+          p1 += sCA[j] > 0 ? uj : -uj;
+          p2 += sCA[j] * uj;
+        }
+        const T coeff1 = warp_sum(p1);
+        const T coeff2 = warp_sum(p2);
+        const T coeff3 = normX - constraint;
+        T step_max2;
+        if (mode == 2) {
+          step_max2 = C - constraint;
+        } else if (mode == 1) {
+          const T delta = coeff2 * coeff2 - coeff1 * coeff3;
+          step_max2 = delta < 0 ? INF : (coeff2 - sqrt(delta)) / coeff1;
+          step_max2 = ref_min(C, step_max2);
+        } else {
+          step_max2 = coeff1 < 0 ? INF : (constraint - thrs) / coeff1;
+          step_max2 = ref_min(C, step_max2);
+        }
+        step = ref_min(ref_min(step, step_max2), step_max);
+        if (step == INF) break;
+
+        // ---- updates
+        for (int j = lane; j <= i; j += 32) {
+          T c = sCoef[j] + step * sU[j];
+          if (pos && c < 0) c = 0;
+          sCoef[j] = c;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const int r0 = v * 128 + lane * 4;
+          Vec4<T> d = ld4(sDtR + r0);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) d.v[e] += (-step) * A[v][e];
+          st4(sDtR + r0, d);
+        }
+        normX += coeff1 * step * step - 2 * coeff2 * step;
+        thrs += step * coeff1;
+        __syncwarp();
+        if (path)
+          for (int k = lane; k <= i; k += 32)
+            path[(size_t)iter * K + sInd[k]] = sCoef[k];
+
+        if (step == step_max) {
+          // ---- drop atom first_zero, downdate invGs
+          const int fz = first_zero;
+          const int rd = sInd[fz];
+          if (lane == own_lane(rd)) act &= ~(1u << own_bit(rd));
+          --cnt;
+          const T schur = sInv[(size_t)fz * ldi + fz];
+          for (int r = lane; r < i; r += 32)
+            sW[r] = sInv[(size_t)(r < fz ? r : r + 1) * ldi + fz];
+          for (int j0 = fz; j0 < i; j0 += 32) {
+            const int j = j0 + lane;
+            int ti = 0;
+            T tc = 0;
+            if (j < i) { ti = sInd[j + 1]; tc = sCoef[j + 1]; }
+            __syncwarp();
+            if (j < i) { sInd[j] = ti; sCoef[j] = tc; }
+            __syncwarp();
+          }
+          if (lane == 0) { sInd[i] = -1; sCoef[i] = 0; }
+          __syncwarp();
+          const T alpha = T(-1) / schur;
+          for (int r = 0; r < i; ++r) {
+            const T* src = sInv + (size_t)(r < fz ? r : r + 1) * ldi;
+            T* dst = sInv + (size_t)r * ldi;
+            const T wr = sW[r];
+            for (int c0 = 0; c0 < i; c0 += 32) {
+              const int c = c0 + lane;
+              T val = 0;
+              if (c < i) {
+                const T wc = sW[c];
+                const T whi = c > r ? wc : wr;
+                const T wlo = c > r ? wr : wc;
+                val = src[c < fz ? c : c + 1] + (alpha * whi) * wlo;
+              }
+              __syncwarp();
+              if (c < i) dst[c] = val;
+              __syncwarp();
+            }
+          }
+          newAtom = false;
+          i -= 2;
+        } else {
+          newAtom = true;
+        }
+        if ((iter >= length_path - 1) || fabs(step) < 1e-15 || step == step_max2 ||
+            (normX < 1e-15) || (i == (L - 1)) ||
+            (mode == 1 && normX - constraint < 1e-15) ||
+            (mode == 0 && (constraint - thrs < 1e-15)))
+          break;
+      }
+    }
+    __syncwarp();
+
+    // ---- output: active set sorted by atom index
+    if (overflow) {
+      if (lane == 0) {
+        const int slot = atomicAdd(a.overflow_count, 1);
+        a.overflow_list[slot] = sig;
+        a.out_cnt[sig] = 0;
+      }
+    } else {
+      int* oind = a.out_ind + (size_t)sig * a.L;
+      T* oval = a.out_val + (size_t)sig * a.L;
+      for (int j = lane; j < cnt; j += 32) {
+        const int me = sInd[j];
+        int rank = 0;
+        for (int k = 0; k < cnt; ++k) rank += sInd[k] < me;
+        oind[rank] = me;
+        oval[rank] = sCoef[j];
+      }
+      if (lane == 0) a.out_cnt[sig] = cnt;
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T>
+size_t lars_smem_per_warp(int Kp, int Lcap) { return lars_state_bytes(Kp, Lcap, sizeof(T)); }
+
+template <typename T, int NV>
+static cudaError_t launch_nv(const LarsArgs<T>& a, int grid, int warps_per_block,
+                             size_t smem, cudaStream_t st) {
+  auto k = lars_kernel<T, NV>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, warps_per_block * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_lars(const LarsArgs<T>& a, int grid, int warps_per_block, cudaStream_t st) {
+  const size_t smem = a.gstate ? 0 : (size_t)warps_per_block * lars_state_bytes(a.Kp, a.Lcap, sizeof(T));
+  switch (a.Kp / 128) {
+    case 1: return launch_nv<T, 1>(a, grid, warps_per_block, smem, st);
+    case 2: return launch_nv<T, 2>(a, grid, warps_per_block, smem, st);
+    case 3: return launch_nv<T, 3>(a, grid, warps_per_block, smem, st);
+    case 4: return launch_nv<T, 4>(a, grid, warps_per_block, smem, st);
+    case 5: return launch_nv<T, 5>(a, grid, warps_per_block, smem, st);
+    case 6: return launch_nv<T, 6>(a, grid, warps_per_block, smem, st);
+    case 7: return launch_nv<T, 7>(a, grid, warps_per_block, smem, st);
+    case 8: return launch_nv<T, 8>(a, grid, warps_per_block, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+int lars_max_warps_per_sm(int Kp) {
+  const void* fn = nullptr;
+  switch (Kp / 128) {
+    case 1: fn = (const void*)lars_kernel<T, 1>; break;
+    case 2: fn = (const void*)lars_kernel<T, 2>; break;
+    case 3: fn = (const void*)lars_kernel<T, 3>; break;
+    case 4: fn = (const void*)lars_kernel<T, 4>; break;
+    case 5: fn = (const void*)lars_kernel<T, 5>; break;
+    case 6: fn = (const void*)lars_kernel<T, 6>; break;
+    case 7: fn = (const void*)lars_kernel<T, 7>; break;
+    case 8: fn = (const void*)lars_kernel<T, 8>; break;
+    default: return 0;
+  }
+  cudaFuncAttributes attr;
+  if (cudaFuncGetAttributes(&attr, fn) != cudaSuccess) return 0;
+  const int regs = attr.numRegs > 0 ? attr.numRegs : 64;
+  return 65536 / (regs * 32);
+}
+
+template cudaError_t launch_lars<float>(const LarsArgs<float>&, int, int, cudaStream_t);
+template cudaError_t launch_lars<double>(const LarsArgs<double>&, int, int, cudaStream_t);
+template int lars_max_warps_per_sm<float>(int);
+template int lars_max_warps_per_sm<double>(int);
+
+}  // namespace sc

@@ -1,0 +1,124 @@
+"""ctypes bindings of libspams_b200.so (the C ABI in include/spams_b200.h).
+
+The library is loaded from spams-devel_b200/lib/ (built in-tree by
+spams-devel_b200/build.py).  There is no CPU fallback: a missing library is an
+ImportError, a missing GPU an error status from every coding call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libspams_b200.so")
+
+SC_OK = 0
+SC_ERR_INVALID_ARG = 1
+SC_ERR_DIMENSIONS = 2
+SC_ERR_NO_CRITERION = 3
+SC_ERR_CUDA = 4
+SC_ERR_OUT_OF_MEMORY = 5
+SC_ERR_NO_DEVICE = 6
+SC_ERR_CAPACITY = 7
+SC_ERR_TIMEOUT = 8
+SC_ERR_UNSUPPORTED = 9
+
+SC_L1COEFFS, SC_L2ERROR, SC_PENALTY = 0, 1, 2
+SC_PREC_FP32, SC_PREC_BF16X3 = 0, 1
+
+# every entry point the header declares (checked by the CPU test suite)
+EXPORTS = (
+    "sc_version", "sc_last_error", "sc_device_count", "sc_csc_free_f32", "sc_csc_free_f64",
+    "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
+    "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
+)
+
+
+class CscF32(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
+                ("colptr", C.POINTER(C.c_int64)), ("rows", C.POINTER(C.c_int32)),
+                ("vals", C.POINTER(C.c_float))]
+
+
+class CscF64(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
+                ("colptr", C.POINTER(C.c_int64)), ("rows", C.POINTER(C.c_int32)),
+                ("vals", C.POINTER(C.c_double))]
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("reserved", C.c_int * 6)]
+
+
+class ScError(RuntimeError):
+    """A non-OK status from the engine; `.status` holds the sc_status code."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(msg)
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python spams-devel_b200/build.py` "
+            "(the engine has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    p = C.c_void_p
+    i32, i64 = C.c_int, C.c_int64
+    f32p, f64p = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    i32p, i64p = C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    f, d = C.c_float, C.c_double
+    opt = C.POINTER(Options)
+    sigs = {
+        "sc_version": (C.c_char_p, []),
+        "sc_last_error": (C.c_char_p, []),
+        "sc_device_count": (i32, [C.POINTER(C.c_int)]),
+        "sc_csc_free_f32": (None, [C.POINTER(CscF32)]),
+        "sc_csc_free_f64": (None, [C.POINTER(CscF64)]),
+        "sc_release_all": (None, []),
+        "sc_omp_f32": (i32, [f32p, i32, i64, f32p, i32, i32p, i64, f32p, i64, f32p, i64, i32,
+                             f32p, opt, C.POINTER(CscF32)]),
+        "sc_omp_f64": (i32, [f64p, i32, i64, f64p, i32, i32p, i64, f64p, i64, f64p, i64, i32,
+                             f64p, opt, C.POINTER(CscF64)]),
+        "sc_lasso_f32": (i32, [f32p, i32, i64, f32p, i32, i32, f, f, i32, i32, i32, i32, i32, i32,
+                               f32p, opt, C.POINTER(CscF32)]),
+        "sc_lasso_f64": (i32, [f64p, i32, i64, f64p, i32, i32, d, d, i32, i32, i32, i32, i32, i32,
+                               f64p, opt, C.POINTER(CscF64)]),
+        "sc_lasso_gram_f32": (i32, [f32p, i32, i64, f32p, i32, f32p, i32, f, f, i32, i32, i32, i32,
+                                    f32p, opt, C.POINTER(CscF32)]),
+        "sc_lasso_gram_f64": (i32, [f64p, i32, i64, f64p, i32, f64p, i32, d, d, i32, i32, i32, i32,
+                                    f64p, opt, C.POINTER(CscF64)]),
+        "sc_omp_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, p, p, p, p, p, p, i64, i64p, p,
+                                 opt]),
+        "sc_lasso_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, i32, i32, i32, p, p, p, i64,
+                                   i64p, p, opt]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    s = lib().sc_last_error()
+    return s.decode() if s else ""
+
+
+def check(status: int) -> None:
+    if status != SC_OK:
+        raise ScError(status, last_error())
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    st = lib().sc_device_count(C.byref(c))
+    return c.value if st == SC_OK else 0
