@@ -74,8 +74,25 @@ typedef struct {
 typedef struct {
   int precision;  /* SC_PREC_* (single precision calls only); default FP32 */
   int device;     /* CUDA device ordinal; default 0 */
-  int reserved[6];
+  int profile;    /* nonzero: time each stage with CUDA events and count the
+                     coding steps (the call then synchronises its stream) */
+  int reserved[5];
 } sc_options;
+
+/* What the calling thread's last coding call did on the device.  Stage times
+ * are filled only when that call ran with sc_options.profile set. */
+typedef struct {
+  double ms_gram;      /* Gram matrix D^T D (+ ridge) */
+  double ms_norms;     /* ||x_i||^2 */
+  double ms_corr;      /* correlations D^T X */
+  double ms_code;      /* OMP / LARS kernels, overflow rerun included */
+  double ms_csc;       /* CSC scan and gather */
+  double ms_total;     /* first to last stage event */
+  int64_t launches;    /* engine kernels launched by the call */
+  int64_t signals;     /* signals coded */
+  int64_t steps;       /* OMP / LARS steps summed over the signals (profile) */
+  int64_t overflowed;  /* signals rerun with global-memory state (profile) */
+} sc_profile;
 
 /* ---- library / status ------------------------------------------------- */
 const char* sc_version(void);
@@ -85,6 +102,8 @@ void sc_csc_free_f32(sc_csc_f32* a);      /* frees colptr/rows/vals, zeroes the 
 void sc_csc_free_f64(sc_csc_f64* a);
 /* Releases the engine's cached device workspaces and streams on all devices. */
 void sc_release_all(void);
+/* Copies the calling thread's last-call profile (see sc_profile). */
+sc_status sc_last_profile(sc_profile* out);
 
 /* ---- OMP ----------------------------------------------------------------
  * Replaces _omp<T> (cpp_library/spams.h:250-293) -> omp<T>

@@ -121,6 +121,52 @@ void release_all() {
 }
 
 // ---------------------------------------------------------------------------
+// per-call profile (stage events when requested, launch counts always)
+static thread_local sc_profile g_prof;
+
+enum { ST_GRAM = 0, ST_NORMS, ST_CORR, ST_CODE, ST_CSC, ST_OTHER, ST_N };
+
+struct Prof {
+  bool on = false;
+  cudaStream_t st = nullptr;
+  std::vector<cudaEvent_t> evs;
+  std::vector<int> stage;  // stage that starts at evs[i]
+  void mark(int s) {
+    if (!on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, st);
+    evs.push_back(e);
+    stage.push_back(s);
+  }
+  void launches(int k) { g_prof.launches += k; }
+  void finish() {
+    if (!on || evs.empty()) return;
+    cudaEventSynchronize(evs.back());
+    double acc[ST_N] = {0};
+    for (size_t i = 0; i + 1 < evs.size(); ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, evs[i], evs[i + 1]);
+      acc[stage[i]] += ms;
+    }
+    float tot = 0;
+    cudaEventElapsedTime(&tot, evs.front(), evs.back());
+    g_prof.ms_gram += acc[ST_GRAM];
+    g_prof.ms_norms += acc[ST_NORMS];
+    g_prof.ms_corr += acc[ST_CORR];
+    g_prof.ms_code += acc[ST_CODE];
+    g_prof.ms_csc += acc[ST_CSC];
+    g_prof.ms_total += tot;
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    evs.clear();
+    stage.clear();
+  }
+  ~Prof() { for (cudaEvent_t e : evs) cudaEventDestroy(e); }
+};
+
+static void prof_reset() { memset(&g_prof, 0, sizeof(g_prof)); }
+
+// ---------------------------------------------------------------------------
 // launch shapes
 struct Shape {
   int Lcap;   // active-set capacity in shared memory
@@ -176,7 +222,7 @@ struct HostSink {
 
 template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
-                              HostSink<T>* sink, int* d_capflag) {
+                              HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
   const Shape shp = pick_shape<T>(c, p.lars, Kp, p.L);
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
@@ -215,6 +261,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
 
   unsigned* d_counter = reinterpret_cast<unsigned*>(c.misc.ptr);   // [0], [1]
   int* d_ovf_count = reinterpret_cast<int*>(c.misc.ptr) + 4;         // [4]
+  unsigned long long* d_steps =
+      pr.on ? reinterpret_cast<unsigned long long*>(c.misc.ptr) + 24 : nullptr;  // bytes 192..199
+  if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
+  g_prof.signals += p.n;
 
   int64_t nnz_total = 0;
   for (int64_t start = 0; start < p.n; start += nc) {
@@ -223,6 +273,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     T* norms = reinterpret_cast<T*>(c.norms.ptr);
     // ---- inputs: ||x||^2 and D^T x
     const T* xchunk = nullptr;
+    pr.mark(ST_OTHER);
     if (p.hX) {
       SC_CUDA(cudaMemcpyAsync(c.xstage.ptr, p.hX + (size_t)start * p.m,
                               (size_t)cn * p.m * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -230,13 +281,17 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     } else {
       xchunk = p.dX + (size_t)start * p.m;
     }
+    pr.mark(ST_NORMS);
     SC_CUDA(launch_colnorms<T>(xchunk, p.m, cn, norms, st));
+    pr.mark(ST_CORR);
     if (p.dDtX)
       SC_CUDA(launch_pad_rows<T>(p.dDtX + (size_t)start * p.K, p.K, p.K, cn, dtx, Kp, st));
     else
       SC_CUDA(launch_gemm_tn<T>(p.dD, p.m, p.K, xchunk, p.m, cn, p.m, dtx, Kp, Kp, st));
+    pr.launches(2);
     // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
     SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
+    pr.mark(ST_CODE);
     int* cnt = reinterpret_cast<int*>(c.cnt.ptr);
     int* sind = reinterpret_cast<int*>(c.slab_ind.ptr);
     T* sval = reinterpret_cast<T*>(c.slab_val.ptr);
@@ -249,9 +304,11 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.length_path = p.length_path; a.n_jobs = (int)cn; a.n_jobs_dev = nullptr;
       a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
       a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
-      a.gstate = nullptr; a.path = path;
+      a.gstate = nullptr; a.path = path; a.steps = d_steps;
       SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
+      pr.launches(1);
       if (may_overflow) {
+        pr.launches(1);
         a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
         a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
         a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
@@ -267,16 +324,25 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.n_jobs = (int)cn; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
       a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
       a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
-      a.path = path;
+      a.path = path; a.steps = d_steps;
       SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
+      pr.launches(1);
       if (may_overflow) {
+        pr.launches(1);
         a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
         a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
         a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
         SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
       }
     }
+    if (pr.on && may_overflow) {
+      SC_CUDA(cudaMemcpyAsync(c.pinned_small, d_ovf_count, 4, cudaMemcpyDeviceToHost, st));
+      SC_CUDA(cudaStreamSynchronize(st));
+      g_prof.overflowed += *reinterpret_cast<int*>(c.pinned_small);
+    }
     // ---- CSC
+    pr.mark(ST_CSC);
+    pr.launches(4);
     int64_t* scratch = reinterpret_cast<int64_t*>(c.scan.ptr);
     if (sink) {
       int64_t* ccol = reinterpret_cast<int64_t*>(c.ccolptr.ptr);
@@ -307,6 +373,13 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                                    p.d_rows, p.d_vals, st));
     }
   }
+  pr.mark(ST_OTHER);
+  if (d_steps) {
+    SC_CUDA(cudaMemcpyAsync(c.pinned_small, d_steps, 8, cudaMemcpyDeviceToHost, st));
+    SC_CUDA(cudaStreamSynchronize(st));
+    g_prof.steps += (int64_t)*reinterpret_cast<unsigned long long*>(c.pinned_small);
+  }
+  pr.finish();
   return SC_OK;
 }
 
@@ -357,6 +430,12 @@ struct CallGuard {
   ~CallGuard() { cudaEventRecord(c->last_use, st); }
 };
 
+static sc_status check_opts(const sc_options* opt) {
+  if (opt && opt->precision != SC_PREC_FP32)
+    return fail(SC_ERR_UNSUPPORTED, "precision mode %d is not available in this build", opt->precision);
+  return SC_OK;
+}
+
 static sc_status check_kp(int K) {
   if (pad128(K) > 1024)
     return fail(SC_ERR_UNSUPPORTED, "dictionaries with more than 1024 atoms are not supported yet (K=%d)", K);
@@ -397,15 +476,21 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
   SC_TRY(check_kp(K));
 
+  SC_TRY(check_opts(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
   cudaStream_t st = c->stream;
+  Prof pr;
+  pr.on = opt && opt->profile;
+  pr.st = st;
   const int Kp = pad128(K);
   SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
+  pr.mark(ST_GRAM);
   SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, T(0), (T*)c->G.ptr, st));
+  pr.launches(2);
   // per-signal vectors
   const size_t vbytes = (vecL ? 4 * (size_t)n : 0) + (vecE ? sizeof(T) * (size_t)n : 0) +
                         (vecLa ? sizeof(T) * (size_t)n : 0) + 64;
@@ -437,7 +522,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   HostSink<T> sink;
-  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag));
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   if (path)
     SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * scalar_L,
                             cudaMemcpyDeviceToHost, st));
@@ -484,10 +569,14 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (n == 0) return emit_empty<T>(K, 0, out);
   SC_TRY(check_kp(K));
 
+  SC_TRY(check_opts(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
   cudaStream_t st = c->stream;
+  Prof pr;
+  pr.on = opt && opt->profile;
+  pr.st = st;
   const int Kp = pad128(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   Problem<T> p;
@@ -506,20 +595,26 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
     SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
     SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
     const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);  // MAX(lambda2, 1e-10)
+    pr.mark(ST_GRAM);
     SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, ridge, (T*)c->G.ptr, st));
+    pr.launches(2);
     p.dD = (const T*)c->D.ptr;
   }
   p.hX = X; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
+  // coreLARS2 replaces a path length <= 1 by 4L (decomp/decomp.h:1722) and
+  // writes that many columns; the device buffer covers them, only the
+  // caller's max_length_path columns are returned.
+  const int dev_cols = max_length_path <= 1 ? 4 * std::min(L, K) : max_length_path;
   if (path && max_length_path > 0) {
-    SC_TRY(c->path.reserve(sizeof(T) * (size_t)K * max_length_path));
-    SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * max_length_path, st));
+    SC_TRY(c->path.reserve(sizeof(T) * (size_t)K * dev_cols));
+    SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * dev_cols, st));
     p.d_path = (T*)c->path.ptr;
   }
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   HostSink<T> sink;
-  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag));
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   if (p.d_path)
     SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * max_length_path,
                             cudaMemcpyDeviceToHost, st));
@@ -555,10 +650,14 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   if (mode < 0 || mode > 2) return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
   SC_TRY(check_kp(K));
+  SC_TRY(check_opts(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
   CallGuard g(c, st);
+  Prof pr;
+  pr.on = opt && opt->profile;
+  pr.st = st;
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
@@ -569,12 +668,14 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   const int Kp = pad128(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
+  pr.mark(ST_GRAM);
   SC_CUDA(launch_gram<T>(dD, m, K, Kp, ridge, (T*)c->G.ptr, st));
+  pr.launches(2);
   Problem<T> p;
   p.lars = true; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
-  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag));
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
 }
 
@@ -587,10 +688,14 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
     return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
   SC_TRY(check_kp(K));
+  SC_TRY(check_opts(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
   CallGuard g(c, st);
+  Prof pr;
+  pr.on = opt && opt->profile;
+  pr.st = st;
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
@@ -602,12 +707,14 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   }
   const int Kp = pad128(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
+  pr.mark(ST_GRAM);
   SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));
+  pr.launches(2);
   Problem<T> p;
   p.lars = false; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.Lsig = Lsig; p.eps = eps; p.lambda = lambda; p.dLv = d_L; p.dEps = d_eps; p.dLam = d_lambda;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
-  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag));
+  SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
 }
 
@@ -646,11 +753,18 @@ void sc_csc_free_f64(sc_csc_f64* a) {
 }
 void sc_release_all(void) { sc::release_all(); }
 
+sc_status sc_last_profile(sc_profile* out) {
+  if (!out) return fail(SC_ERR_INVALID_ARG, "null profile");
+  *out = sc::g_prof;
+  return SC_OK;
+}
+
 sc_status sc_omp_f32(const float* X, int m, int64_t n, const float* D, int K, const int* L,
                      int64_t nL, const float* eps, int64_t nEps, const float* lambda,
                      int64_t nLambda, int numThreads, float* path, const sc_options* opt,
                      sc_csc_f32* out) {
   (void)numThreads;
+  prof_reset();
   return omp_host<float>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out);
 }
 sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K, const int* L,
@@ -658,6 +772,7 @@ sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K, 
                      int64_t nLambda, int numThreads, double* path, const sc_options* opt,
                      sc_csc_f64* out) {
   (void)numThreads;
+  prof_reset();
   return omp_host<double>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out);
 }
 
@@ -666,6 +781,7 @@ sc_status sc_lasso_f32(const float* X, int m, int64_t n, const float* D, int K, 
                        int max_length_path, int cholesky, float* path, const sc_options* opt,
                        sc_csc_f32* out) {
   (void)numThreads;
+  prof_reset();
   return lasso_host<float>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos, ols,
                            max_length_path, cholesky, path, opt, out);
 }
@@ -674,6 +790,7 @@ sc_status sc_lasso_f64(const double* X, int m, int64_t n, const double* D, int K
                        int numThreads, int max_length_path, int cholesky, double* path,
                        const sc_options* opt, sc_csc_f64* out) {
   (void)numThreads;
+  prof_reset();
   return lasso_host<double>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos,
                             ols, max_length_path, cholesky, path, opt, out);
 }
@@ -685,6 +802,7 @@ sc_status sc_lasso_gram_f32(const float* X, int m, int64_t n, const float* Q, in
   (void)numThreads;
   if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
   static const float dummy = 0;
+  prof_reset();
   return lasso_host<float>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
                            pos, 0, max_length_path, 0, path, opt, out);
 }
@@ -695,6 +813,7 @@ sc_status sc_lasso_gram_f64(const double* X, int m, int64_t n, const double* Q, 
   (void)numThreads;
   if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
   static const double dummy = 0;
+  prof_reset();
   return lasso_host<double>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
                             pos, 0, max_length_path, 0, path, opt, out);
 }
@@ -704,6 +823,7 @@ sc_status sc_omp_f32_dev(const float* dX, int m, int64_t n, const float* dD, int
                          const float* d_lambda, int64_t* d_colptr, int32_t* d_rows,
                          float* d_vals, int64_t cap, int64_t* nnz_out, void* stream,
                          const sc_options* opt) {
+  prof_reset();
   return omp_dev<float>(dX, m, n, dD, K, L, eps, lambda, d_L, d_eps, d_lambda, d_colptr, d_rows,
                         d_vals, cap, nnz_out, stream, opt);
 }
@@ -712,6 +832,7 @@ sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD, i
                            float lambda1, float lambda2, int mode, int pos, int max_length_path,
                            int64_t* d_colptr, int32_t* d_rows, float* d_vals, int64_t cap,
                            int64_t* nnz_out, void* stream, const sc_options* opt) {
+  prof_reset();
   return lasso_dev<float>(dX, m, n, dD, K, L, lambda1, lambda2, mode, pos, max_length_path,
                           d_colptr, d_rows, d_vals, cap, nnz_out, stream, opt);
 }

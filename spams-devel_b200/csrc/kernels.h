@@ -48,6 +48,7 @@ struct LarsArgs {
   int* overflow_count;
   T* gstate;           // NULL: state in shared memory; else per-warp global slabs
   T* path;             // K x length_path for signal 0, or NULL
+  unsigned long long* steps;  // if set: total homotopy steps are added here
 };
 
 template <typename T>
@@ -74,6 +75,7 @@ struct OmpArgs {
   int* overflow_count;
   T* gstate;
   T* path;             // K x L for signal 0, or NULL
+  unsigned long long* steps;  // if set: total OMP steps are added here
 };
 
 template <typename T>

@@ -84,13 +84,14 @@ lars_kernel(const LarsArgs<T> a) {
       for (int e = 0; e < 4; ++e) {
         const int r = r0 + e;
         if (r < K) {
-          const T key = pos ? d.v[e] : fabs(d.v[e]);
+          T key = pos ? d.v[e] : fabs(d.v[e]);
+          if (key != key) key = -INF;
           if (key > bkey || (key == bkey && r < bidx)) { bkey = key; bidx = r; }
         }
       }
     }
     warp_argmax(bkey, bidx);
-    int cur = bidx;
+    int cur = __shfl_sync(kFull, bidx, 0);
     T normX = a.norms[sig];
     for (int j = lane; j < Lc; j += 32) sCoef[j] = 0;  // coeffs.setZeros()
     __syncwarp();
@@ -105,9 +106,9 @@ lars_kernel(const LarsArgs<T> a) {
     }
 
     uint32_t act = 0;  // active flags of this lane's rows
+    int iter = 0;
     if (!skip) {
       bool newAtom = true;
-      int iter = 0;
       T thrs = 0;
       for (int i = 0; i < L; ++i) {
         ++iter;
@@ -170,8 +171,9 @@ lars_kernel(const LarsArgs<T> a) {
           if (ratio > 0 && ratio <= zkey) { zkey = ratio; zidx = r; }
         }
         warp_argmin_last(zkey, zidx);
-        const T step_max = zkey;
-        const int first_zero = zidx;
+        // lane 0's result drives the (warp-uniform) control flow
+        const T step_max = __shfl_sync(kFull, zkey, 0);
+        const int first_zero = __shfl_sync(kFull, zidx, 0);
         __syncwarp();
         const T C = fabs(sCA[0]);
 
@@ -211,7 +213,9 @@ lars_kernel(const LarsArgs<T> a) {
                 if (!pos && aa > T(-1)) c1 = (d.v[e] + C) / (T(1) + aa);
                 if (aa < T(1)) c2 = (C - d.v[e]) / (T(1) - aa);
               }
-              const T k1 = fabs(c1), k2 = fabs(c2);
+              T k1 = fabs(c1), k2 = fabs(c2);
+              if (k1 != k1) k1 = INF;  // NaN never wins (cblas_iamin skips it)
+              if (k2 != k2) k2 = INF;
               if (k1 < mkey || (k1 == mkey && r < midx)) { mkey = k1; midx = r; mval = c1; }
               if (k2 < mkey || (k2 == mkey && r + K < midx)) { mkey = k2; midx = r + K; mval = c2; }
             }
@@ -224,8 +228,8 @@ lars_kernel(const LarsArgs<T> a) {
           const T v2 = __shfl_xor_sync(kFull, mval, o);
           if (k2 < mkey || (k2 == mkey && i2 < midx)) { mkey = k2; midx = i2; mval = v2; }
         }
-        T step = mval;
-        cur = midx % K;
+        T step = __shfl_sync(kFull, mval, 0);
+        cur = __shfl_sync(kFull, midx, 0) % K;
 
         // ---- polynomial of normX along the step
         T p1 = 0, p2 = 0;
@@ -325,6 +329,7 @@ lars_kernel(const LarsArgs<T> a) {
     }
     __syncwarp();
 
+    if (a.steps && lane == 0 && !overflow) atomicAdd(a.steps, (unsigned long long)iter);
     // ---- output: active set sorted by atom index
     if (overflow) {
       if (lane == 0) {

@@ -73,13 +73,14 @@ omp_kernel(const OmpArgs<T> a) {
       for (int e = 0; e < 4; ++e) {
         const int r = r0 + e;
         if (r < K) {
-          const T key = fabs(d.v[e]);
+          T key = fabs(d.v[e]);
+          if (key != key) key = -1;  // NaN never wins
           if (key > bkey || (key == bkey && r < bidx)) { bkey = key; bidx = r; }
         }
       }
     }
     warp_argmax(bkey, bidx);
-    int c = bidx;
+    int c = __shfl_sync(kFull, bidx, 0);
     __syncwarp();
 
     int j = 0;
@@ -162,7 +163,8 @@ omp_kernel(const OmpArgs<T> a) {
             if (r < K) {
               T sc = (rd.v[e] * rd.v[e]) / nm.v[e];
               if ((act >> (v * 4 + e)) & 1u) sc = 0;
-              const T key = fabs(sc);
+              T key = fabs(sc);
+              if (key != key) key = -1;
               if (key > bkey || (key == bkey && r < bidx)) { bkey = key; bidx = r; }
             }
           }
@@ -170,12 +172,13 @@ omp_kernel(const OmpArgs<T> a) {
           st4(sNorm + r0, nm);
         }
         warp_argmax(bkey, bidx);
-        c = bidx;
+        c = __shfl_sync(kFull, bidx, 0);
         __syncwarp();
       }
     }
     __syncwarp();
 
+    if (a.steps && lane == 0 && !overflow) atomicAdd(a.steps, (unsigned long long)j);
     if (overflow) {
       if (lane == 0) {
         const int slot = atomicAdd(a.overflow_count, 1);

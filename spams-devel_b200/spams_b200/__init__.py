@@ -11,7 +11,7 @@ GPU.  `omp_device` / `lasso_device` take CUDA tensors and leave the CSC on the
 device.
 """
 from ._lib import (SC_L1COEFFS, SC_L2ERROR, SC_PENALTY, SC_PREC_BF16X3, SC_PREC_FP32,  # noqa: F401
-                   ScError, device_count, lib, last_error)
+                   ScError, device_count, last_error, last_profile, lib)
 from .api import lasso, lasso_device, omp, omp_device  # noqa: F401
 
 L1COEFFS, L2ERROR, PENALTY = SC_L1COEFFS, SC_L2ERROR, SC_PENALTY

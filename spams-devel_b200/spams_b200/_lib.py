@@ -31,6 +31,7 @@ EXPORTS = (
     "sc_version", "sc_last_error", "sc_device_count", "sc_csc_free_f32", "sc_csc_free_f64",
     "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
     "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
+    "sc_last_profile",
 )
 
 
@@ -47,7 +48,18 @@ class CscF64(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("reserved", C.c_int * 6)]
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("profile", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms_gram", C.c_double), ("ms_norms", C.c_double), ("ms_corr", C.c_double),
+                ("ms_code", C.c_double), ("ms_csc", C.c_double), ("ms_total", C.c_double),
+                ("launches", C.c_int64), ("signals", C.c_int64), ("steps", C.c_int64),
+                ("overflowed", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ScError(RuntimeError):
@@ -83,6 +95,7 @@ def lib() -> C.CDLL:
         "sc_csc_free_f32": (None, [C.POINTER(CscF32)]),
         "sc_csc_free_f64": (None, [C.POINTER(CscF64)]),
         "sc_release_all": (None, []),
+        "sc_last_profile": (i32, [C.POINTER(Profile)]),
         "sc_omp_f32": (i32, [f32p, i32, i64, f32p, i32, i32p, i64, f32p, i64, f32p, i64, i32,
                              f32p, opt, C.POINTER(CscF32)]),
         "sc_omp_f64": (i32, [f64p, i32, i64, f64p, i32, i32p, i64, f64p, i64, f64p, i64, i32,
@@ -116,6 +129,13 @@ def last_error() -> str:
 def check(status: int) -> None:
     if status != SC_OK:
         raise ScError(status, last_error())
+
+
+def last_profile() -> dict:
+    """Profile of this thread's last coding call (stage times need profile=1)."""
+    p = Profile()
+    check(lib().sc_last_profile(C.byref(p)))
+    return p.as_dict()
 
 
 def device_count() -> int:

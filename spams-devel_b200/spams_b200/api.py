@@ -36,10 +36,11 @@ def _ptr(a: Optional[np.ndarray], ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
-def _opts(precision: Optional[int], device: int) -> Options:
+def _opts(precision: Optional[int], device: int, profile: bool = False) -> Options:
     o = Options()
     o.precision = SC_PREC_FP32 if precision is None else int(precision)
     o.device = int(device)
+    o.profile = int(bool(profile))
     return o
 
 
@@ -170,7 +171,8 @@ def _clamp_lasso_L(m: int, K: int, L: int, lambda1: float, lambda2: float, mode:
 
 
 def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
-                 max_length_path=-1, stream=None, precision=None, out=None, sync=True):
+                 max_length_path=-1, stream=None, precision=None, out=None, sync=True,
+                 profile=False):
     """LARS-Lasso with X (m x n) and D (m x K) as column-major float32 CUDA
     tensors (i.e. the .t() views of row-major n x m / K x m tensors, or any
     tensor whose column j is contiguous).  Returns (colptr, rows, vals, nnz)
@@ -190,7 +192,7 @@ def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
     colptr, rows, vals = out
     nnz = C.c_int64(0)
     s = stream if stream is not None else torch.cuda.current_stream(X.device)
-    o = _opts(precision, X.device.index or 0)
+    o = _opts(precision, X.device.index or 0, profile)
     st = _lib.lib().sc_lasso_f32_dev(
         C.c_void_p(X.data_ptr()), m, n, C.c_void_p(D.data_ptr()), K, int(L), float(lambda1),
         float(lambda2), int(mode), int(bool(pos)), int(max_length_path),
@@ -201,7 +203,8 @@ def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
 
 
 def omp_device(X, D, L=None, eps=None, lambda1=None, L_vec=None, eps_vec=None,
-               lambda_vec=None, stream=None, precision=None, out=None, sync=True):
+               lambda_vec=None, stream=None, precision=None, out=None, sync=True,
+               profile=False):
     """OMP with CUDA tensors (see lasso_device).  Scalars L / eps / lambda1
     follow the facade defaults; *_vec are optional per-signal CUDA tensors
     (int32 / float32) of n entries, with L then the maximum of L_vec."""
@@ -225,7 +228,7 @@ def omp_device(X, D, L=None, eps=None, lambda1=None, L_vec=None, eps_vec=None,
     colptr, rows, vals = out
     nnz = C.c_int64(0)
     s = stream if stream is not None else torch.cuda.current_stream(X.device)
-    o = _opts(precision, X.device.index or 0)
+    o = _opts(precision, X.device.index or 0, profile)
 
     def vp(t):
         return C.c_void_p(t.data_ptr()) if t is not None else None
