@@ -30,8 +30,30 @@ __device__ __forceinline__ int own_bit(int r) { return ((r >> 7) << 2) | (r & 3)
 // MIN macro of linalg/utils.h:46.
 template <typename T> __device__ __forceinline__ T ref_min(T a, T b) { return a > b ? b : a; }
 
+// Screening division: approximate in single precision (a few ulp), exact in
+// double precision.
+__device__ __forceinline__ float fast_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fast_div(double a, double b) { return a / b; }
+
+// Dot product of a shared-memory row with a vector, four accumulators.
+template <typename T>
+__device__ __forceinline__ T dot_row(const T* __restrict__ row, const T* __restrict__ x, int n) {
+  T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int c = 0;
+  for (; c + 4 <= n; c += 4) {
+    s0 += row[c] * x[c];
+    s1 += row[c + 1] * x[c + 1];
+    s2 += row[c + 2] * x[c + 2];
+    s3 += row[c + 3] * x[c + 3];
+  }
+  for (; c < n; ++c) s0 += row[c] * x[c];
+  return (s0 + s1) + (s2 + s3);
+}
+
+// Single precision: three 8-warp blocks per SM (80 registers); double
+// precision keeps two so that its wider row state stays in registers.
 template <typename T, int NV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 lars_kernel(const LarsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -125,12 +147,7 @@ lars_kernel(const LarsArgs<T> a) {
             if (lane == 0) sInv[0] = T(1) / sG[0];
           } else {
             // w = invGs(0:i,0:i) g(0:i)
-            for (int r = lane; r < i; r += 32) {
-              T s = 0;
-              const T* row = sInv + (size_t)r * ldi;
-              for (int c = 0; c < i; ++c) s += row[c] * sG[c];
-              sW[r] = s;
-            }
+            for (int r = lane; r < i; r += 32) sW[r] = dot_row(sInv + (size_t)r * ldi, sG, i);
             __syncwarp();
             T part = 0;
             for (int r = lane; r < i; r += 32) part += sW[r] * sG[r];
@@ -163,9 +180,7 @@ lars_kernel(const LarsArgs<T> a) {
         T zkey = INF;
         int zidx = -1;
         for (int r = lane; r <= i; r += 32) {
-          T s = 0;
-          const T* row = sInv + (size_t)r * ldi;
-          for (int c = 0; c <= i; ++c) s += row[c] * sS[c];
+          const T s = dot_row(sInv + (size_t)r * ldi, sS, i + 1);
           sU[r] = s;
           const T ratio = -sCoef[r] / s;
           if (ratio > 0 && ratio <= zkey) { zkey = ratio; zidx = r; }
@@ -195,9 +210,19 @@ lars_kernel(const LarsArgs<T> a) {
           }
         }
 
-        // ---- joining steps: first minimum magnitude over the 2K candidates
-        T mkey = INF, mval = INF;
-        int midx = 0x7fffffff;
+        // ---- joining steps: first minimum magnitude over the 2K candidates.
+        // A candidate is a fraction num/den with den > 0; fractions are
+        // compared by cross-multiplication (no division), in four independent
+        // chains (one per row offset e) to keep the comparisons off one long
+        // dependency chain.  Each lane's winner is then divided exactly and
+        // the warp reduces the exact (|value|, index) pairs: ties go to the
+        // first index as in cblas_iamin.  Infinite candidates (active atoms,
+        // |A_j| beyond the bounds) never decide a step (the step is then
+        // step_max or step_max2).
+        T cn[4], cd[4];
+        int ci[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) { cn[e] = INF; cd[e] = T(1); ci[e] = 0x7fffffff; }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const int r0 = v * 128 + lane * 4;
@@ -205,22 +230,35 @@ lars_kernel(const LarsArgs<T> a) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int r = r0 + e;
-            if (r < K) {
-              const bool active = (act >> (v * 4 + e)) & 1u;
-              const T aa = A[v][e];
-              T c1 = INF, c2 = INF;
-              if (!active && aa < INF) {
-                if (!pos && aa > T(-1)) c1 = (d.v[e] + C) / (T(1) + aa);
-                if (aa < T(1)) c2 = (C - d.v[e]) / (T(1) - aa);
-              }
-              T k1 = fabs(c1), k2 = fabs(c2);
-              if (k1 != k1) k1 = INF;  // NaN never wins (cblas_iamin skips it)
-              if (k2 != k2) k2 = INF;
-              if (k1 < mkey || (k1 == mkey && r < midx)) { mkey = k1; midx = r; mval = c1; }
-              if (k2 < mkey || (k2 == mkey && r + K < midx)) { mkey = k2; midx = r + K; mval = c2; }
+            const bool active = (act >> (v * 4 + e)) & 1u;
+            const T aa = A[v][e];
+            const bool ok = r < K && !active && aa < INF;
+            if (ok && !pos && aa > T(-1)) {
+              const T num = d.v[e] + C, den = T(1) + aa;
+              const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
+              if (lhs < rhs || (lhs == rhs && r < ci[e])) { cn[e] = num; cd[e] = den; ci[e] = r; }
+            }
+            if (ok && aa < T(1)) {
+              const T num = C - d.v[e], den = T(1) - aa;
+              const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
+              if (lhs < rhs || (lhs == rhs && r + K < ci[e])) { cn[e] = num; cd[e] = den; ci[e] = r + K; }
             }
           }
         }
+#pragma unroll
+        for (int h = 1; h < 4; h <<= 1) {
+#pragma unroll
+          for (int e = 0; e + h < 4; e += 2 * h) {
+            const T lhs = fabs(cn[e + h]) * cd[e], rhs = fabs(cn[e]) * cd[e + h];
+            if (lhs < rhs || (lhs == rhs && ci[e + h] < ci[e])) {
+              cn[e] = cn[e + h]; cd[e] = cd[e + h]; ci[e] = ci[e + h];
+            }
+          }
+        }
+        int midx = ci[0];
+        T mval = cn[0] / cd[0];
+        T mkey = fabs(mval);
+        if (!(mkey < INF)) { mkey = INF; mval = INF; }  // NaN never wins
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           const T k2 = __shfl_xor_sync(kFull, mkey, o);
@@ -361,6 +399,8 @@ static cudaError_t launch_nv(const LarsArgs<T>& a, int grid, int warps_per_block
                              size_t smem, cudaStream_t st) {
   auto k = lars_kernel<T, NV>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   k<<<grid, warps_per_block * 32, smem, st>>>(a);
   return cudaGetLastError();

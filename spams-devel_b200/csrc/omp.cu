@@ -21,7 +21,7 @@
 namespace sc {
 
 template <typename T, int NV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 omp_kernel(const OmpArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -145,10 +145,13 @@ omp_kernel(const OmpArgs<T> a) {
             for (int e = 0; e < 4; ++e) A[v][e] += g.v[e] * ul;
           }
         }
-        // ---- residual correlations, norms, scores; next choice
+        // ---- residual correlations, norms, scores; next choice (first index
+        // of the largest |score|, four independent chains merged at the end)
         const T mRU = -sRUn[j];
-        bkey = -1;
-        bidx = 0x7fffffff;
+        T ck[4];
+        int cix[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) { ck[e] = -1; cix[e] = 0x7fffffff; }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const int r0 = v * 128 + lane * 4;
@@ -164,13 +167,23 @@ omp_kernel(const OmpArgs<T> a) {
               T sc = (rd.v[e] * rd.v[e]) / nm.v[e];
               if ((act >> (v * 4 + e)) & 1u) sc = 0;
               T key = fabs(sc);
-              if (key != key) key = -1;
-              if (key > bkey || (key == bkey && r < bidx)) { bkey = key; bidx = r; }
+              if (key != key) key = -1;  // NaN never wins
+              if (key > ck[e]) { ck[e] = key; cix[e] = r; }  // rows ascend per chain
             }
           }
           st4(sRdn + r0, rd);
           st4(sNorm + r0, nm);
         }
+#pragma unroll
+        for (int h = 1; h < 4; h <<= 1)
+#pragma unroll
+          for (int e = 0; e + h < 4; e += 2 * h)
+            if (ck[e + h] > ck[e] || (ck[e + h] == ck[e] && cix[e + h] < cix[e])) {
+              ck[e] = ck[e + h];
+              cix[e] = cix[e + h];
+            }
+        bkey = ck[0];
+        bidx = cix[0];
         warp_argmax(bkey, bidx);
         c = __shfl_sync(kFull, bidx, 0);
         __syncwarp();
@@ -218,6 +231,8 @@ template <typename T, int NV>
 static cudaError_t launch_nv(const OmpArgs<T>& a, int grid, int wpb, size_t smem, cudaStream_t st) {
   auto k = omp_kernel<T, NV>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   k<<<grid, wpb * 32, smem, st>>>(a);
   return cudaGetLastError();
