@@ -251,8 +251,8 @@ def run_ours(args) -> None:
     nnz = int(outs[0][n].item())
 
     # ---- timed region B: per-stage device times of the same call
-    stage = {"ms_gram": 0.0, "ms_norms": 0.0, "ms_corr": 0.0, "ms_code": 0.0, "ms_csc": 0.0,
-             "steps": 0, "overflowed": 0}
+    stage = {"ms_gram": 0.0, "ms_norms": 0.0, "ms_corr": 0.0, "ms_code": 0.0, "ms_refine": 0.0,
+             "ms_csc": 0.0, "steps": 0, "overflowed": 0}
     for i in range(args.steps):
         flush.fill_(float(i))
         step(profile=True)
@@ -321,7 +321,8 @@ def run_ours(args) -> None:
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
                      "traffic": traffic, "peak_source": peaks["source"],
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
-        "stages_ms": {k: stage[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code", "ms_csc")},
+        "stages_ms": {k: stage[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
+                                            "ms_refine", "ms_csc")},
         "homotopy_steps_per_signal": stage["steps"] / n,
         "nnz_per_signal": nnz / n,
         "overflowed_signals": stage["overflowed"],

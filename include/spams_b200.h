@@ -49,8 +49,9 @@ enum { SC_L1COEFFS = 0, SC_L2ERROR = 1, SC_PENALTY = 2 };
 /* Numerical form of the correlation / Gram products.
  *   SC_PREC_FP32: plain FP32 products (CUDA cores), FP32 iterations.
  *   SC_PREC_BF16X3: tcgen05 tensor-core products from a BF16 hi/lo split
- *                   (hi*hi + hi*lo + lo*hi, FP32 accumulate), FP32 iterations,
- *                   FP64 refinement of the final active-set coefficients.
+ *                   (hi*hi + hi*lo + lo*hi, FP32 accumulate), FP32 iterations;
+ *                   with sc_options.refine, FP64 refinement of the final
+ *                   active-set coefficients.
  * Double-precision entry points always compute in FP64. */
 enum { SC_PREC_FP32 = 0, SC_PREC_BF16X3 = 1 };
 
@@ -76,7 +77,10 @@ typedef struct {
   int device;     /* CUDA device ordinal; default 0 */
   int profile;    /* nonzero: time each stage with CUDA events and count the
                      coding steps (the call then synchronises its stream) */
-  int reserved[5];
+  int refine;     /* > 0: refine the final single-precision coefficients in
+                     FP64 on their active sets (from D, X and the Gram);
+                     default off */
+  int reserved[4];
 } sc_options;
 
 /* What the calling thread's last coding call did on the device.  Stage times
@@ -86,6 +90,7 @@ typedef struct {
   double ms_norms;     /* ||x_i||^2 */
   double ms_corr;      /* correlations D^T X */
   double ms_code;      /* OMP / LARS kernels, overflow rerun included */
+  double ms_refine;    /* FP64 refinement of the final coefficients (BF16X3) */
   double ms_csc;       /* CSC scan and gather */
   double ms_total;     /* first to last stage event */
   int64_t launches;    /* engine kernels launched by the call */
@@ -178,6 +183,15 @@ sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD,
                            int32_t* d_rows, float* d_vals, int64_t cap,
                            int64_t* nnz_out, void* stream,
                            const sc_options* opt);
+
+/* ---- products -----------------------------------------------------------
+ * Correlations C = D^T X (K x n, column-major, ld ldc >= K) of device arrays,
+ * in the numerical form `precision` (SC_PREC_FP32 or SC_PREC_BF16X3): the
+ * product the coding calls compute first.  Replaces ProdMatrix<T>'s D^T X
+ * (linalg/linalg.h:1021-1067, 5101-5190; Matrix::mult with transA).
+ * Asynchronous on `stream`. */
+sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_t n,
+                          float* dC, int ldc, int precision, void* stream);
 
 #ifdef __cplusplus
 }  /* extern "C" */

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/spams_b200.h"
@@ -124,7 +125,7 @@ void release_all() {
 // per-call profile (stage events when requested, launch counts always)
 static thread_local sc_profile g_prof;
 
-enum { ST_GRAM = 0, ST_NORMS, ST_CORR, ST_CODE, ST_CSC, ST_OTHER, ST_N };
+enum { ST_GRAM = 0, ST_NORMS, ST_CORR, ST_CODE, ST_REFINE, ST_CSC, ST_OTHER, ST_N };
 
 struct Prof {
   bool on = false;
@@ -155,6 +156,7 @@ struct Prof {
     g_prof.ms_norms += acc[ST_NORMS];
     g_prof.ms_corr += acc[ST_CORR];
     g_prof.ms_code += acc[ST_CODE];
+    g_prof.ms_refine += acc[ST_REFINE];
     g_prof.ms_csc += acc[ST_CSC];
     g_prof.ms_total += tot;
     for (cudaEvent_t e : evs) cudaEventDestroy(e);
@@ -211,6 +213,12 @@ struct Problem {
   int64_t* d_colptr = nullptr; int32_t* d_rows = nullptr; T* d_vals = nullptr;
   int64_t cap = 0;
   T* d_path = nullptr;            // device path of signal 0 (zeroed), or nullptr
+  // BF16 hi/lo tensor-core correlations + FP64 refinement (float only)
+  bool tc = false;
+  bool refine = false;            // FP64 refinement of the final coefficients
+  const void* dDsplit = nullptr;  // Dhi (mp x K bf16) followed by Dlo
+  int mp = 0;                     // m rounded up to the 64-element k-block
+  int* d_tc_err = nullptr;
 };
 
 template <typename T>
@@ -227,7 +235,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   const Shape shp = pick_shape<T>(c, p.lars, Kp, p.L);
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
   const size_t per_sig = (size_t)Kp * sizeof(T) + (size_t)p.L * (sizeof(T) + 4) + 64 +
-                         (p.hX ? (size_t)p.m * sizeof(T) : 0) +
+                         (p.hX ? (size_t)p.m * sizeof(T) : 0) + (p.tc ? (size_t)p.mp * 4 : 0) +
                          (sink ? (size_t)p.L * (sizeof(T) + 4) + 8 : 0);
   int64_t nc = (int64_t)std::max<size_t>(4096, ((size_t)2 << 30) / per_sig);
   nc = std::min<int64_t>(nc, std::max<int64_t>(p.n, 1));
@@ -243,6 +251,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   const int64_t scan_len = scan_scratch_len(nc);
   SC_TRY(c.scan.reserve((size_t)scan_len * 8));
   if (p.hX) SC_TRY(c.xstage.reserve((size_t)nc * p.m * sizeof(T)));
+  if (p.tc) SC_TRY(c.xsplit.reserve((size_t)nc * p.mp * 4));
+  SC_TRY(c.level.reserve((size_t)nc * sizeof(T)));
   if (sink) {
     SC_TRY(c.ccolptr.reserve((size_t)(nc + 1) * 8));
     SC_TRY(c.crows.reserve((size_t)nc * p.L * 4));
@@ -284,11 +294,23 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     pr.mark(ST_NORMS);
     SC_CUDA(launch_colnorms<T>(xchunk, p.m, cn, norms, st));
     pr.mark(ST_CORR);
-    if (p.dDtX)
+    if (p.dDtX) {
       SC_CUDA(launch_pad_rows<T>(p.dDtX + (size_t)start * p.K, p.K, p.K, cn, dtx, Kp, st));
-    else
+      pr.launches(2);
+    } else if (p.tc) {
+      if constexpr (std::is_same<T, float>::value) {
+        char* xs = reinterpret_cast<char*>(c.xsplit.ptr);
+        const size_t half = (size_t)p.mp * cn * 2;
+        SC_CUDA(launch_bf16_split(xchunk, p.m, p.m, cn, p.mp, xs, xs + half, st));
+        const char* ds = reinterpret_cast<const char*>(p.dDsplit);
+        SC_CUDA(launch_tc_corr(ds, ds + (size_t)p.mp * p.K * 2, p.K, xs, xs + half, cn, p.mp, 3,
+                               dtx, Kp, Kp, p.d_tc_err, st));
+        pr.launches(3);
+      }
+    } else {
       SC_CUDA(launch_gemm_tn<T>(p.dD, p.m, p.K, xchunk, p.m, cn, p.m, dtx, Kp, Kp, st));
-    pr.launches(2);
+      pr.launches(2);
+    }
     // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
     SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
     pr.mark(ST_CODE);
@@ -305,6 +327,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
       a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
       a.gstate = nullptr; a.path = path; a.steps = d_steps;
+      a.out_level = p.refine ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
       SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
       pr.launches(1);
       if (may_overflow) {
@@ -333,6 +356,15 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
         a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
         SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
+      }
+    }
+    if (p.refine && p.dD) {
+      if constexpr (std::is_same<T, float>::value) {
+        pr.mark(ST_REFINE);
+        SC_CUDA(launch_refine(p.dD, p.m, xchunk, dG, Kp, sind, sval, p.L, cnt,
+                              p.lars ? reinterpret_cast<const float*>(c.level.ptr) : nullptr, cn,
+                              st));
+        pr.launches(1);
       }
     }
     if (pr.on && may_overflow) {
@@ -430,9 +462,47 @@ struct CallGuard {
   ~CallGuard() { cudaEventRecord(c->last_use, st); }
 };
 
+// Single-precision calls take SC_PREC_FP32 or SC_PREC_BF16X3; double
+// precision calls always compute in FP64 and ignore the field.
+template <typename T>
 static sc_status check_opts(const sc_options* opt) {
-  if (opt && opt->precision != SC_PREC_FP32)
-    return fail(SC_ERR_UNSUPPORTED, "precision mode %d is not available in this build", opt->precision);
+  if (!opt || !std::is_same<T, float>::value) return SC_OK;
+  if (opt->precision != SC_PREC_FP32 && opt->precision != SC_PREC_BF16X3)
+    return fail(SC_ERR_INVALID_ARG, "unknown precision mode %d", opt->precision);
+  if (opt->precision == SC_PREC_BF16X3 && !tc_gemm_available())
+    return fail(SC_ERR_UNSUPPORTED, "BF16x3 products need the CUDA driver's tensor-map encoder");
+  return SC_OK;
+}
+
+static bool want_tc(const sc_options* opt) { return opt && opt->precision == SC_PREC_BF16X3; }
+static bool want_refine(const sc_options* opt) { return opt && opt->refine > 0; }
+
+// Splits D into its BF16 hi / lo halves for the tensor-core products.
+template <typename T>
+static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& pr) {
+  if constexpr (std::is_same<T, float>::value) {
+    p.tc = true;
+    p.mp = tc_pad_m(p.m);
+    SC_TRY(c.dsplit.reserve((size_t)p.mp * p.K * 4));
+    SC_TRY(c.misc.reserve(256));
+    p.d_tc_err = reinterpret_cast<int*>(c.misc.ptr) + 48;
+    SC_CUDA(cudaMemsetAsync(p.d_tc_err, 0, 4, st));
+    char* ds = reinterpret_cast<char*>(c.dsplit.ptr);
+    SC_CUDA(launch_bf16_split(p.dD, p.m, p.m, p.K, p.mp, ds, ds + (size_t)p.mp * p.K * 2, st));
+    pr.launches(1);
+    p.dDsplit = ds;
+  }
+  return SC_OK;
+}
+
+// After the stream has drained: a tensor-core pipeline wait that gave up.
+template <typename T>
+static sc_status check_tc(DeviceCtx& c, cudaStream_t st, const Problem<T>& p) {
+  if (!p.tc) return SC_OK;
+  int* h = reinterpret_cast<int*>(c.pinned_small) + 16;
+  SC_CUDA(cudaMemcpyAsync(h, p.d_tc_err, 4, cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaStreamSynchronize(st));
+  if (*h) return fail(SC_ERR_TIMEOUT, "tensor-core correlation pipeline: a bounded wait gave up");
   return SC_OK;
 }
 
@@ -476,7 +546,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
   SC_TRY(check_kp(K));
 
-  SC_TRY(check_opts(opt));
+  SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
@@ -522,7 +592,10 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   HostSink<T> sink;
+  if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  p.refine = want_refine(opt) && std::is_same<T, float>::value;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
+  SC_TRY(check_tc<T>(*c, st, p));
   if (path)
     SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * scalar_L,
                             cudaMemcpyDeviceToHost, st));
@@ -569,7 +642,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (n == 0) return emit_empty<T>(K, 0, out);
   SC_TRY(check_kp(K));
 
-  SC_TRY(check_opts(opt));
+  SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
@@ -614,7 +687,10 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   SC_TRY(c->misc.reserve(256));
   int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
   HostSink<T> sink;
+  if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  p.refine = want_refine(opt) && std::is_same<T, float>::value;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
+  SC_TRY(check_tc<T>(*c, st, p));
   if (p.d_path)
     SC_CUDA(cudaMemcpyAsync(path, c->path.ptr, sizeof(T) * (size_t)K * max_length_path,
                             cudaMemcpyDeviceToHost, st));
@@ -650,7 +726,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   if (mode < 0 || mode > 2) return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
   SC_TRY(check_kp(K));
-  SC_TRY(check_opts(opt));
+  SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
@@ -675,7 +751,10 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   p.lars = true; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
+  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  p.refine = want_refine(opt) && std::is_same<T, float>::value;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
+  if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
 }
 
@@ -688,7 +767,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
     return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
   SC_TRY(check_kp(K));
-  SC_TRY(check_opts(opt));
+  SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
@@ -714,7 +793,10 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   p.lars = false; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.Lsig = Lsig; p.eps = eps; p.lambda = lambda; p.dLv = d_L; p.dEps = d_eps; p.dLam = d_lambda;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
+  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  p.refine = want_refine(opt) && std::is_same<T, float>::value;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
+  if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
 }
 
@@ -826,6 +908,41 @@ sc_status sc_omp_f32_dev(const float* dX, int m, int64_t n, const float* dD, int
   prof_reset();
   return omp_dev<float>(dX, m, n, dD, K, L, eps, lambda, d_L, d_eps, d_lambda, d_colptr, d_rows,
                         d_vals, cap, nnz_out, stream, opt);
+}
+
+sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_t n, float* dC,
+                          int ldc, int precision, void* stream) {
+  prof_reset();
+  if (m <= 0 || K <= 0 || n < 0 || ldc < K || !dD || !dX || (n > 0 && !dC))
+    return fail(SC_ERR_INVALID_ARG, "corr : bad arguments");
+  DeviceCtx* c = nullptr;
+  SC_TRY(get_ctx(0, &c));
+  cudaStream_t st = (cudaStream_t)stream;
+  CallGuard g(c, st);
+  if (n == 0) return SC_OK;
+  if (precision == SC_PREC_FP32) {
+    SC_CUDA(launch_gemm_tn<float>(dD, m, K, dX, m, n, m, dC, ldc, K, st));
+    return SC_OK;
+  }
+  if (precision != SC_PREC_BF16X3) return fail(SC_ERR_UNSUPPORTED, "corr : precision %d", precision);
+  if (!tc_gemm_available()) return fail(SC_ERR_UNSUPPORTED, "corr : tensor-map encoder unavailable");
+  const int mp = tc_pad_m(m);
+  SC_TRY(c->D.reserve((size_t)mp * K * 4));  // hi + lo
+  SC_TRY(c->xstage.reserve((size_t)mp * n * 4));
+  SC_TRY(c->misc.reserve(256));
+  int* d_err = reinterpret_cast<int*>(c->misc.ptr) + 48;
+  char* dh = (char*)c->D.ptr;
+  char* xh = (char*)c->xstage.ptr;
+  SC_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+  SC_CUDA(launch_bf16_split(dD, m, m, K, mp, dh, dh + (size_t)mp * K * 2, st));
+  SC_CUDA(launch_bf16_split(dX, m, m, n, mp, xh, xh + (size_t)mp * n * 2, st));
+  SC_CUDA(launch_tc_corr(dh, dh + (size_t)mp * K * 2, K, xh, xh + (size_t)mp * n * 2, n, mp, 3,
+                         dC, ldc, K, d_err, st));
+  int* h = reinterpret_cast<int*>(c->pinned_small);
+  SC_CUDA(cudaMemcpyAsync(h, d_err, 4, cudaMemcpyDeviceToHost, st));
+  SC_CUDA(cudaStreamSynchronize(st));
+  if (*h) return fail(SC_ERR_TIMEOUT, "corr : tensor-core pipeline wait timed out");
+  return SC_OK;
 }
 
 sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD, int K, int L,

@@ -49,6 +49,7 @@ struct LarsArgs {
   T* gstate;           // NULL: state in shared memory; else per-warp global slabs
   T* path;             // K x length_path for signal 0, or NULL
   unsigned long long* steps;  // if set: total homotopy steps are added here
+  T* out_level;        // if set: n correlation levels of the final active sets
 };
 
 template <typename T>
@@ -106,6 +107,17 @@ template <typename T>
 cudaError_t launch_pad_rows(const T* src, int K, int64_t ldsrc, int64_t n, T* dst,
                             int Kp, cudaStream_t st);
 
+// ---- FP64 refinement of the final coefficients ----------------------------
+// For every signal with a non-empty active set A (sorted atom indices and
+// coefficients in the slabs) recompute, in double precision,
+//     a_A = G_AA^{-1} (D_A^T x - level * sign(a_A))     (lasso, level per signal)
+//     a_A = G_AA^{-1}  D_A^T x                          (OMP: level == NULL)
+// with D_A^T x from the float32 inputs; active sets beyond 32 atoms keep
+// their values.
+cudaError_t launch_refine(const float* D, int m, const float* X, const float* G, int Kp,
+                          const int* slab_ind, float* slab_val, int L, const int* cnt,
+                          const float* level, int64_t n, cudaStream_t st);
+
 // ---- CSC assembly ----------------------------------------------------------
 // colptr[i+1] = base + cnt[0] + ... + cnt[i]; with base == NULL the base is 0
 // and colptr[0] is written as 0, otherwise colptr[0] is left alone (it is
@@ -123,5 +135,17 @@ cudaError_t launch_csc_gather(const int* slab_ind, const T* slab_val, int L,
 
 // ---- BF16 hi/lo split tensor-core products (sm_100a tcgen05) --------------
 bool tc_gemm_available();
+// rows of the bf16 split operands: m rounded up to the 64-element k-block
+int tc_pad_m(int m);
+// x (rows x cols fp32, ld ldx) -> hi / lo bf16 (rows_pad x cols), zero padded
+cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t cols, int rows_pad,
+                              void* hi, void* lo, cudaStream_t st);
+// C = sum over the first `nterms` of (Dhi,Xhi), (Dhi,Xlo), (Dlo,Xhi) of
+// D^T X on tcgen05: rows 0..rows_out-1 (rows_out <= K rounded up to 128;
+// rows beyond K come out zero) of each of the n columns (ld ldc).  *err is
+// set when a bounded wait gave up.
+cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* Xhi,
+                           const void* Xlo, int64_t n, int m_pad, int nterms, float* C, int ldc,
+                           int rows_out, int* err, cudaStream_t st);
 
 }  // namespace sc

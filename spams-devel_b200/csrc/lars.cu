@@ -85,6 +85,13 @@ lars_kernel(const LarsArgs<T> a) {
   const bool pos = a.pos != 0;
 
   const int n_jobs = a.n_jobs_dev ? *a.n_jobs_dev : a.n_jobs;
+  // rows r >= K (padding up to Kp) never join: mark them active once
+  uint32_t pad_act = 0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (v * 128 + lane * 4 + e >= K) pad_act |= 1u << (v * 4 + e);
   for (;;) {
     int job = 0;
     if (lane == 0) job = (int)atomicAdd(a.work_counter, 1u);
@@ -127,8 +134,10 @@ lars_kernel(const LarsArgs<T> a) {
       if (mode == 1 && normX < constraint) skip = true;
     }
 
-    uint32_t act = 0;  // active flags of this lane's rows
+    uint32_t act = pad_act;  // active flags of this lane's rows (+ padding rows)
     int iter = 0;
+    T c_end = 0;        // correlation level of the active set at exit
+    bool at_lambda = false;
     if (!skip) {
       bool newAtom = true;
       T thrs = 0;
@@ -191,6 +200,7 @@ lars_kernel(const LarsArgs<T> a) {
         const int first_zero = __shfl_sync(kFull, zidx, 0);
         __syncwarp();
         const T C = fabs(sCA[0]);
+        c_end = C;
 
         // ---- A = Ga u
         T A[NV][4];
@@ -232,7 +242,7 @@ lars_kernel(const LarsArgs<T> a) {
             const int r = r0 + e;
             const bool active = (act >> (v * 4 + e)) & 1u;
             const T aa = A[v][e];
-            const bool ok = r < K && !active && aa < INF;
+            const bool ok = !active && aa < INF;  // padding rows are marked active
             if (ok && !pos && aa > T(-1)) {
               const T num = d.v[e] + C, den = T(1) + aa;
               const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
@@ -309,6 +319,8 @@ lars_kernel(const LarsArgs<T> a) {
         }
         normX += coeff1 * step * step - 2 * coeff2 * step;
         thrs += step * coeff1;
+        c_end = C - step;
+        at_lambda = step == step_max2;
         __syncwarp();
         if (path)
           for (int k = lane; k <= i; k += 32)
@@ -385,7 +397,11 @@ lars_kernel(const LarsArgs<T> a) {
         oind[rank] = me;
         oval[rank] = sCoef[j];
       }
-      if (lane == 0) a.out_cnt[sig] = cnt;
+      if (lane == 0) {
+        a.out_cnt[sig] = cnt;
+        // the level the final coefficients satisfy G_AA a = c_A - level s_A
+        if (a.out_level) a.out_level[sig] = (mode == 2 && at_lambda) ? constraint : c_end;
+      }
     }
     __syncwarp();
   }

@@ -1,0 +1,317 @@
+// Correlations C = D^T X on the 5th-generation tensor cores (sm_100a):
+// BF16 hi/lo split operands, FP32 accumulation in tensor memory.
+//
+//   x = hi(x) + lo(x), hi = bf16(x), lo = bf16(x - hi)
+//   C = Dhi^T Xhi + Dhi^T Xlo + Dlo^T Xhi        (the lo*lo term is dropped)
+//
+// The three products are one GEMM over a reduction dimension of 3 m_pad: the
+// k-block loop walks the three (A, B) operand pairs in turn.  Operands are
+// K-major (the signal dimension m is contiguous in both D and X), staged by
+// TMA into 128-byte-swizzled shared-memory tiles, multiplied by tcgen05.mma
+// (M = 128 atoms, N = 128 signals, K = 16) issued by one thread, accumulated
+// in TMEM and read back by four warps with tcgen05.ld for a column-major
+// store of C (atoms contiguous per signal, the layout the coding kernels
+// read).  Every mbarrier wait is bounded: on timeout the CTA records an error,
+// drains its own copies, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace sc {
+
+constexpr int TC_BM = 128;          // atoms per tile (MMA M)
+constexpr int TC_BN = 128;          // signals per tile (MMA N)
+constexpr int TC_BK = 64;           // bf16 per 128-byte swizzled row
+constexpr int TC_STAGES = 3;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;
+constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
+constexpr int TC_TMEM_COLS = 128;   // fp32 accumulator columns (= TC_BN)
+constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr long long TC_TIMEOUT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+// Wait for the phase of the given parity to complete; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > TC_TIMEOUT_CYCLES) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand in 128-byte swizzled rows,
+// 8-row core-matrix groups 1024 bytes apart (tile base 1024-byte aligned).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address
+  d |= (uint64_t)1u << 16;                            // leading offset (unused for SW128 K-major)
+  d |= (uint64_t)(1024u >> 4) << 32;                  // stride offset: 8 rows x 128 B
+  d |= (uint64_t)1u << 46;                            // descriptor version (sm_100)
+  d |= (uint64_t)2u << 61;                            // swizzle mode: 128 B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B, both
+// K-major, M = TC_BM, N = TC_BN.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                            ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(128, 1)
+tc_corr_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+               const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+               float* __restrict__ C, int ldc, int rows_out, int64_t n, int m_pad, int nterms,
+               int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
+  // bars[0..S) full, bars[S..2S) empty, bars[2S] accumulator ready
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * TC_STAGES + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * TC_BM;
+  const int64_t n0 = (int64_t)blockIdx.y * TC_BN;
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (TC_STAGES + s); };
+  const uint32_t acc_bar = bar0 + 8u * (2 * TC_STAGES);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(acc_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int kb_per_term = m_pad / TC_BK;
+  const int total_kb = nterms * kb_per_term;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer
+    int issued = 0;
+    for (int kb = 0; kb < total_kb; ++kb) {
+      const int s = kb % TC_STAGES;
+      const uint32_t round = kb / TC_STAGES;
+      if (*abort_flag || !mbar_wait(empty_bar(s), (round & 1u) ^ 1u)) { *abort_flag = 1; break; }
+      const int term = kb / kb_per_term;
+      const int kx = (kb % kb_per_term) * TC_BK;
+      const CUtensorMap* ma = term == 2 ? &mAl : &mAh;
+      const CUtensorMap* mb = term == 1 ? &mBl : &mBh;
+      uint8_t* st = smem + (size_t)s * TC_STAGE_BYTES;
+      mbar_expect_tx(full_bar(s), TC_STAGE_BYTES);
+      tma_load_2d(smem_u32(st), ma, full_bar(s), kx, m0);
+      tma_load_2d(smem_u32(st + TC_A_BYTES), mb, full_bar(s), kx, (int)n0);
+      issued = kb + 1;
+    }
+    if (*abort_flag) {
+      // drain: every issued stage whose completion was not observed by the
+      // MMA thread lands before the CTA may exit
+      for (int kb = issued - TC_STAGES < 0 ? 0 : issued - TC_STAGES; kb < issued; ++kb)
+        mbar_wait(full_bar(kb % TC_STAGES), (uint32_t)(kb / TC_STAGES) & 1u);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    for (int kb = 0; kb < total_kb; ++kb) {
+      const int s = kb % TC_STAGES;
+      const uint32_t round = kb / TC_STAGES;
+      if (*abort_flag || !mbar_wait(full_bar(s), round & 1u)) { *abort_flag = 1; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_addr = smem_u32(smem + (size_t)s * TC_STAGE_BYTES);
+      const uint32_t b_addr = a_addr + TC_A_BYTES;
+#pragma unroll
+      for (int k = 0; k < TC_BK / 16; ++k)
+        umma_bf16(tmem, sw128_desc(a_addr + 32u * k), sw128_desc(b_addr + 32u * k),
+                  (kb > 0 || k > 0) ? 1u : 0u);
+      umma_commit(empty_bar(s));  // stage free once these MMAs have read it
+    }
+    umma_commit(acc_bar);  // accumulator complete (also after an abort)
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM -> registers -> C (column-major, atoms contiguous)
+  const bool acc_ok = mbar_wait(acc_bar, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (acc_ok && !*abort_flag) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+            "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+            "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+            "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < rows_out) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int64_t col = n0 + c0 + j;
+          if (col < n) C[(size_t)col * ldc + row] = __uint_as_float(v[j]);
+        }
+      }
+    }
+  }
+  if ((!acc_ok || *abort_flag) && threadIdx.x == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+}
+
+// x (rows x cols, ld ldx, fp32) -> hi, lo (rows_pad x cols, bf16), zero rows
+// beyond `rows`.
+__global__ void bf16_split_kernel(const float* __restrict__ x, int rows, int64_t ldx, int64_t cols,
+                                  int rows_pad, __nv_bfloat16* __restrict__ hi,
+                                  __nv_bfloat16* __restrict__ lo) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)rows_pad * cols) return;
+  const int r = (int)(idx % rows_pad);
+  const int64_t c = idx / rows_pad;
+  const float v = r < rows ? x[(size_t)c * ldx + r] : 0.f;
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  hi[idx] = h;
+  lo[idx] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// ---------------------------------------------------------------------------
+// host side
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static bool load_encode() {
+  if (g_encode) return true;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return false;
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return true;
+}
+
+// 2-D bf16 tensor of `outer` rows of `inner` contiguous elements; box of
+// 64 x box_rows with 128-byte swizzle, zero fill out of range.
+static bool make_map(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer,
+                     uint32_t box_rows) {
+  if (((uintptr_t)base & 15u) != 0 || (inner * 2) % 16 != 0) return false;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * 2};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool tc_gemm_available() { return load_encode(); }
+
+int tc_pad_m(int m) { return ((m + TC_BK - 1) / TC_BK) * TC_BK; }
+
+cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t cols, int rows_pad,
+                              void* hi, void* lo, cudaStream_t st) {
+  const int64_t tot = (int64_t)rows_pad * cols;
+  if (tot <= 0) return cudaSuccess;
+  bf16_split_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
+      x, rows, ldx, cols, rows_pad, reinterpret_cast<__nv_bfloat16*>(hi),
+      reinterpret_cast<__nv_bfloat16*>(lo));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* Xhi,
+                           const void* Xlo, int64_t n, int m_pad, int nterms, float* C, int ldc,
+                           int rows_out, int* err, cudaStream_t st) {
+  if (n <= 0 || K <= 0) return cudaSuccess;
+  if (!load_encode()) return cudaErrorNotSupported;
+  const int Kp = ((K + TC_BM - 1) / TC_BM) * TC_BM;
+  if (m_pad % TC_BK != 0 || nterms < 1 || nterms > 3 || rows_out > Kp || ldc < rows_out)
+    return cudaErrorInvalidValue;
+  CUtensorMap mAh, mAl, mBh, mBl;
+  if (!make_map(&mAh, Dhi, m_pad, K, TC_BM) || !make_map(&mAl, Dlo, m_pad, K, TC_BM) ||
+      !make_map(&mBh, Xhi, m_pad, n, TC_BN) || !make_map(&mBl, Xlo, m_pad, n, TC_BN))
+    return cudaErrorInvalidValue;
+  const int64_t gy = (n + TC_BN - 1) / TC_BN;
+  if (gy > 65535) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(tc_corr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TC_SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid(Kp / TC_BM, (unsigned)gy);
+  tc_corr_kernel<<<grid, 128, TC_SMEM, st>>>(mAh, mAl, mBh, mBl, C, ldc, rows_out, n, m_pad,
+                                              nterms, err);
+  return cudaGetLastError();
+}
+
+}  // namespace sc

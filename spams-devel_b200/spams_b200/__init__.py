@@ -12,6 +12,6 @@ device.
 """
 from ._lib import (SC_L1COEFFS, SC_L2ERROR, SC_PENALTY, SC_PREC_BF16X3, SC_PREC_FP32,  # noqa: F401
                    ScError, device_count, last_error, last_profile, lib)
-from .api import lasso, lasso_device, omp, omp_device  # noqa: F401
+from .api import corr_device, lasso, lasso_device, omp, omp_device  # noqa: F401
 
 L1COEFFS, L2ERROR, PENALTY = SC_L1COEFFS, SC_L2ERROR, SC_PENALTY

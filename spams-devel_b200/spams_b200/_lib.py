@@ -31,7 +31,7 @@ EXPORTS = (
     "sc_version", "sc_last_error", "sc_device_count", "sc_csc_free_f32", "sc_csc_free_f64",
     "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
     "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
-    "sc_last_profile",
+    "sc_last_profile", "sc_corr_f32_dev",
 )
 
 
@@ -49,12 +49,13 @@ class CscF64(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("profile", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("refine", C.c_int), ("reserved", C.c_int * 4)]
 
 
 class Profile(C.Structure):
     _fields_ = [("ms_gram", C.c_double), ("ms_norms", C.c_double), ("ms_corr", C.c_double),
-                ("ms_code", C.c_double), ("ms_csc", C.c_double), ("ms_total", C.c_double),
+                ("ms_code", C.c_double), ("ms_refine", C.c_double), ("ms_csc", C.c_double),
+                ("ms_total", C.c_double),
                 ("launches", C.c_int64), ("signals", C.c_int64), ("steps", C.c_int64),
                 ("overflowed", C.c_int64)]
 
@@ -112,6 +113,7 @@ def lib() -> C.CDLL:
                                  opt]),
         "sc_lasso_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, i32, i32, i32, p, p, p, i64,
                                    i64p, p, opt]),
+        "sc_corr_f32_dev": (i32, [p, i32, i32, p, i64, p, i32, i32, p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)

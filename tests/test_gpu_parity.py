@@ -203,3 +203,57 @@ def test_per_signal_L_eps_matches_oracle():
     assert rel_err(a, ref) <= 1e-9
     a32 = spams_b200.omp(X.astype(np.float32), D.astype(np.float32), L=L, eps=eps.astype(np.float32))
     assert support_match(a32, ref) >= 0.99
+
+
+# ---------------------------------------------------------------------------
+# BF16 hi/lo tensor-core correlations + FP64 refinement of the final codes
+
+BF16 = spams_b200.SC_PREC_BF16X3
+
+
+def test_bf16x3_lasso_workload_vs_oracle():
+    X, D = W.config_lasso(20000)
+    ref = O.orc_lasso(X, D, lambda1=0.15)
+    a = spams_b200.lasso(X.astype(np.float32), D.astype(np.float32), lambda1=0.15, precision=BF16)
+    assert support_match(a, ref) >= 0.999
+    assert rel_err(a, ref) <= 1e-5
+
+
+def test_bf16x3_omp_plain_workload_vs_oracle():
+    X, D = W.config_omp_small(10000)
+    ref = O.orc_omp(X, D, L=10, eps=0.0)
+    a = spams_b200.omp(X.astype(np.float32), D.astype(np.float32), L=10, eps=0.0, precision=BF16)
+    assert support_match(a, ref) >= 0.999
+    assert rel_err(a, ref) <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["lasso_pen", "lasso_pos", "lasso_l1", "lasso_l2err",
+                                  "lasso_enet", "omp_L10", "omp_eps", "omp_vec"])
+def test_bf16x3_golden(name):
+    g = load_golden(name)
+    a = _gpu_run(g, np.float32, precision=BF16)
+    ref = golden_csc(g, "f64")
+    assert support_match(a, ref) >= 0.99
+    # eps-stopped OMP may take one step more or less on a column whose
+    # residual ends within the correlation error of eps: compare the columns
+    # whose supports agree
+    a, ref = a.tocsc(), ref.tocsc()
+    a.sort_indices()
+    ref.sort_indices()
+    keep = [j for j in range(a.shape[1])
+            if np.array_equal(a.indices[a.indptr[j]:a.indptr[j + 1]],
+                              ref.indices[ref.indptr[j]:ref.indptr[j + 1]])]
+    assert rel_err(a[:, keep], ref[:, keep]) <= 2e-5
+
+
+def test_bf16x3_device_entry_matches_host_entry():
+    import torch
+    X, D = W.config_lasso(5000, seed=3)
+    Xf, Df = X.astype(np.float32), D.astype(np.float32)
+    a = spams_b200.lasso(Xf, Df, lambda1=0.15, precision=BF16)
+    Xt = torch.from_numpy(np.ascontiguousarray(Xf.T)).cuda().t()
+    Dt = torch.from_numpy(np.ascontiguousarray(Df.T)).cuda().t()
+    colptr, rows, vals, nnz = spams_b200.lasso_device(Xt, Dt, 0.15, precision=BF16)
+    assert nnz == a.nnz
+    np.testing.assert_array_equal(rows[:nnz].cpu().numpy(), a.indices)
+    np.testing.assert_array_equal(vals[:nnz].cpu().numpy(), a.data)
