@@ -193,6 +193,25 @@ sc_status sc_lasso_f32_dev(const float* dX, int m, int64_t n, const float* dD,
 sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_t n,
                           float* dC, int ldc, int precision, void* stream);
 
+/* The same BF16 hi/lo tensor-core product (SC_PREC_BF16X3) for callers that
+ * cannot allocate device memory: those that run with a device-memory budget
+ * fixed in advance (a serving process whose own pool already holds the free
+ * memory, where cudaMalloc fails or fragments it) and those that must avoid
+ * the implicit device synchronisation of cudaMalloc / cudaFree.  No counterpart
+ * in the reference (SPAMS allocates its workspaces with new[] on the host).
+ *   The caller passes inputs and output as for sc_corr_f32_dev; the hi / lo
+ *   halves of D and X are staged in a fixed 16 MiB array compiled into the
+ *   library (held on every GPU that loads the library until exit), so
+ *   256 + 4 * m64 * (K + n) bytes must fit in 16 MiB, m64 = m rounded up to a
+ *   multiple of 64 (larger calls return SC_ERR_CAPACITY; split X by columns).
+ *   The first call on a device looks up the array's address there (make it
+ *   before any stream capture).  All calls share the array: calls that
+ *   overlap on the GPU race and must be serialised.  The call returns after
+ *   the stream has finished the product.  No cudaMalloc / cudaFree or other
+ *   allocating routine is called. */
+sc_status sc_corr_bf16x3_noalloc_f32(const float* dD, int m, int K, const float* dX, int64_t n,
+                                     float* dC, int ldc, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -31,7 +31,7 @@ EXPORTS = (
     "sc_version", "sc_last_error", "sc_device_count", "sc_csc_free_f32", "sc_csc_free_f64",
     "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
     "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
-    "sc_last_profile", "sc_corr_f32_dev",
+    "sc_last_profile", "sc_corr_f32_dev", "sc_corr_bf16x3_noalloc_f32",
 )
 
 
@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
         "sc_lasso_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, i32, i32, i32, p, p, p, i64,
                                    i64p, p, opt]),
         "sc_corr_f32_dev": (i32, [p, i32, i32, p, i64, p, i32, i32, p]),
+        "sc_corr_bf16x3_noalloc_f32": (i32, [p, i32, i32, p, i64, p, i32, p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
