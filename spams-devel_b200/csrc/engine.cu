@@ -122,6 +122,21 @@ void release_all() {
 }
 
 // ---------------------------------------------------------------------------
+// Byte offsets inside the per-device 256-byte `misc` buffer.  The first 64
+// bytes (queue heads, overflow count) are cleared before every chunk.
+enum : size_t {
+  MISC_COUNTERS = 0,     // unsigned[2]: work-queue heads (main pass, overflow pass)
+  MISC_OVF_COUNT = 16,   // int: signals sent to the overflow pass
+  MISC_CAPFLAG = 128,    // int: device CSC arrays too small
+  MISC_TC_ERR = 192,     // int: tensor-core pipeline wait gave up
+  MISC_STEPS = 224,      // unsigned long long: coding steps (profile)
+  MISC_BYTES = 256
+};
+template <typename P> static inline P* misc_at(const Buf& b, size_t off) {
+  return reinterpret_cast<P*>(static_cast<char*>(b.ptr) + off);
+}
+
+// ---------------------------------------------------------------------------
 // per-call profile (stage events when requested, launch counts always)
 static thread_local sc_profile g_prof;
 
@@ -247,7 +262,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   SC_TRY(c.slab_val.reserve((size_t)nc * p.L * sizeof(T)));
   SC_TRY(c.cnt.reserve((size_t)nc * 4));
   SC_TRY(c.ovf_list.reserve((size_t)nc * 8));
-  SC_TRY(c.misc.reserve(256));
+  SC_TRY(c.misc.reserve(MISC_BYTES));
   const int64_t scan_len = scan_scratch_len(nc);
   SC_TRY(c.scan.reserve((size_t)scan_len * 8));
   if (p.hX) SC_TRY(c.xstage.reserve((size_t)nc * p.m * sizeof(T)));
@@ -269,10 +284,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   const bool may_overflow = shp.Lcap < p.L;
   if (may_overflow) SC_TRY(c.gstate.reserve((size_t)ovf_grid * ovf_wpb * ovf_per_warp));
 
-  unsigned* d_counter = reinterpret_cast<unsigned*>(c.misc.ptr);   // [0], [1]
-  int* d_ovf_count = reinterpret_cast<int*>(c.misc.ptr) + 4;         // [4]
+  unsigned* d_counter = misc_at<unsigned>(c.misc, MISC_COUNTERS);
+  int* d_ovf_count = misc_at<int>(c.misc, MISC_OVF_COUNT);
   unsigned long long* d_steps =
-      pr.on ? reinterpret_cast<unsigned long long*>(c.misc.ptr) + 24 : nullptr;  // bytes 192..199
+      pr.on ? misc_at<unsigned long long>(c.misc, MISC_STEPS) : nullptr;
   if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
   g_prof.signals += p.n;
 
@@ -484,8 +499,8 @@ static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& 
     p.tc = true;
     p.mp = tc_pad_m(p.m);
     SC_TRY(c.dsplit.reserve((size_t)p.mp * p.K * 4));
-    SC_TRY(c.misc.reserve(256));
-    p.d_tc_err = reinterpret_cast<int*>(c.misc.ptr) + 48;
+    SC_TRY(c.misc.reserve(MISC_BYTES));
+    p.d_tc_err = misc_at<int>(c.misc, MISC_TC_ERR);
     SC_CUDA(cudaMemsetAsync(p.d_tc_err, 0, 4, st));
     char* ds = reinterpret_cast<char*>(c.dsplit.ptr);
     SC_CUDA(launch_bf16_split(p.dD, p.m, p.m, p.K, p.mp, ds, ds + (size_t)p.mp * p.K * 2, st));
@@ -589,8 +604,8 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
     SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * scalar_L, st));
     p.d_path = (T*)c->path.ptr;
   }
-  SC_TRY(c->misc.reserve(256));
-  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_TRY(c->misc.reserve(MISC_BYTES));
+  int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   HostSink<T> sink;
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
@@ -684,8 +699,8 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
     SC_CUDA(cudaMemsetAsync(c->path.ptr, 0, sizeof(T) * (size_t)K * dev_cols, st));
     p.d_path = (T*)c->path.ptr;
   }
-  SC_TRY(c->misc.reserve(256));
-  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_TRY(c->misc.reserve(MISC_BYTES));
+  int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   HostSink<T> sink;
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
@@ -734,8 +749,8 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  SC_TRY(c->misc.reserve(256));
-  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_TRY(c->misc.reserve(MISC_BYTES));
+  int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
   if (n == 0 || L <= 0) {
     SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
@@ -775,8 +790,8 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  SC_TRY(c->misc.reserve(256));
-  int* d_capflag = reinterpret_cast<int*>(c->misc.ptr) + 32;
+  SC_TRY(c->misc.reserve(MISC_BYTES));
+  int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
   // the driver L: with per-signal L the caller passes their maximum as Lsig
   int L = std::min(m, std::min(Lsig, K));
@@ -929,8 +944,8 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
   const int mp = tc_pad_m(m);
   SC_TRY(c->D.reserve((size_t)mp * K * 4));  // hi + lo
   SC_TRY(c->xstage.reserve((size_t)mp * n * 4));
-  SC_TRY(c->misc.reserve(256));
-  int* d_err = reinterpret_cast<int*>(c->misc.ptr) + 48;
+  SC_TRY(c->misc.reserve(MISC_BYTES));
+  int* d_err = misc_at<int>(c->misc, MISC_TC_ERR);
   char* dh = (char*)c->D.ptr;
   char* xh = (char*)c->xstage.ptr;
   SC_CUDA(cudaMemsetAsync(d_err, 0, 4, st));

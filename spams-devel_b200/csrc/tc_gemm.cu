@@ -17,6 +17,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -231,18 +233,38 @@ tc_corr_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ 
 }
 
 // x (rows x cols, ld ldx, fp32) -> hi, lo (rows_pad x cols, bf16), zero rows
-// beyond `rows`.
+// beyond `rows`.  One thread converts 8 consecutive rows of a column (two
+// 16-byte loads when the column is 16-byte aligned, two 16-byte stores).
 __global__ void bf16_split_kernel(const float* __restrict__ x, int rows, int64_t ldx, int64_t cols,
-                                  int rows_pad, __nv_bfloat16* __restrict__ hi,
+                                  int rows_pad, bool vec, __nv_bfloat16* __restrict__ hi,
                                   __nv_bfloat16* __restrict__ lo) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)rows_pad * cols) return;
-  const int r = (int)(idx % rows_pad);
-  const int64_t c = idx / rows_pad;
-  const float v = r < rows ? x[(size_t)c * ldx + r] : 0.f;
-  const __nv_bfloat16 h = __float2bfloat16_rn(v);
-  hi[idx] = h;
-  lo[idx] = __float2bfloat16_rn(v - __bfloat162float(h));
+  const int groups = rows_pad >> 3;
+  const int64_t total = cols * groups;
+  for (int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gid < total;
+       gid += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = gid / groups;
+    const int r0 = (int)(gid - c * groups) << 3;
+    const float* src = x + (size_t)c * ldx + r0;
+    float v[8];
+    if (vec && r0 + 8 <= rows) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+      const float4 b = __ldg(reinterpret_cast<const float4*>(src + 4));
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = r0 + k < rows ? src[k] : 0.f;
+    }
+    __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      h[k] = __float2bfloat16_rn(v[k]);
+      l[k] = __float2bfloat16_rn(v[k] - __bfloat162float(h[k]));
+    }
+    const size_t o = (size_t)c * rows_pad + r0;
+    *reinterpret_cast<uint4*>(hi + o) = *reinterpret_cast<const uint4*>(h);
+    *reinterpret_cast<uint4*>(lo + o) = *reinterpret_cast<const uint4*>(l);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -283,11 +305,15 @@ int tc_pad_m(int m) { return ((m + TC_BK - 1) / TC_BK) * TC_BK; }
 
 cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t cols, int rows_pad,
                               void* hi, void* lo, cudaStream_t st) {
-  const int64_t tot = (int64_t)rows_pad * cols;
+  if (rows_pad % 8 != 0 || ((uintptr_t)hi & 15u) || ((uintptr_t)lo & 15u))
+    return cudaErrorInvalidValue;
+  const int64_t tot = (int64_t)(rows_pad / 8) * cols;
   if (tot <= 0) return cudaSuccess;
-  bf16_split_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
-      x, rows, ldx, cols, rows_pad, reinterpret_cast<__nv_bfloat16*>(hi),
-      reinterpret_cast<__nv_bfloat16*>(lo));
+  const bool vec = (ldx % 4 == 0) && (((uintptr_t)x & 15u) == 0);
+  const int64_t blocks = std::min<int64_t>((tot + 255) / 256, (int64_t)148 * 32);
+  bf16_split_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, rows, ldx, cols, rows_pad, vec,
+                                                      reinterpret_cast<__nv_bfloat16*>(hi),
+                                                      reinterpret_cast<__nv_bfloat16*>(lo));
   return cudaGetLastError();
 }
 

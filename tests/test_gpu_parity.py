@@ -257,3 +257,17 @@ def test_bf16x3_device_entry_matches_host_entry():
     assert nnz == a.nnz
     np.testing.assert_array_equal(rows[:nnz].cpu().numpy(), a.indices)
     np.testing.assert_array_equal(vals[:nnz].cpu().numpy(), a.data)
+
+
+def test_profiled_bf16x3_device_call_reports_no_false_timeout():
+    """Profiling counters and the tensor-core timeout flag live side by side
+    in the engine's small status buffer; a profiled, synchronous BF16x3 call
+    must come back clean and report its steps."""
+    import torch
+    X, D = W.config_lasso(3000, seed=5)
+    Xt = torch.from_numpy(np.ascontiguousarray(X.astype(np.float32).T)).cuda().t()
+    Dt = torch.from_numpy(np.ascontiguousarray(D.astype(np.float32).T)).cuda().t()
+    for _ in range(2):
+        _, _, _, nnz = spams_b200.lasso_device(Xt, Dt, 0.15, precision=BF16, profile=True)
+        p = spams_b200.last_profile()
+        assert nnz > 0 and p["steps"] >= nnz and p["ms_code"] > 0
