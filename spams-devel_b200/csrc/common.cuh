@@ -46,6 +46,33 @@ __device__ __forceinline__ void st4(double* p, const Vec4<double>& q) {
   *reinterpret_cast<double2*>(p + 2) = make_double2(q.v[2], q.v[3]);
 }
 
+// d = a * b + c on a pair of floats with one packed FP32x2 instruction.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rb, {%4, %5};\n\t"
+      "mov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+      "mov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+// Column accumulation acc[0..3] += g[0..3] * u: packed pairs in single
+// precision, plain FMAs in double precision.
+__device__ __forceinline__ void axpy4(float* acc, const Vec4<float>& g, float u) {
+  const float2 uu = make_float2(u, u);
+  const float2 lo = fma2(make_float2(g.v[0], g.v[1]), uu, make_float2(acc[0], acc[1]));
+  const float2 hi = fma2(make_float2(g.v[2], g.v[3]), uu, make_float2(acc[2], acc[3]));
+  acc[0] = lo.x; acc[1] = lo.y; acc[2] = hi.x; acc[3] = hi.y;
+}
+__device__ __forceinline__ void axpy4(double* acc, const Vec4<double>& g, double u) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) acc[e] += g.v[e] * u;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -213,22 +213,21 @@ lars_kernel(const LarsArgs<T> a) {
           const T uj = sU[j];
           const T* gc = a.G + (size_t)sInd[j] * Kp + lane * 4;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            const Vec4<T> g = ldg4(gc + v * 128);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) A[v][e] += g.v[e] * uj;
-          }
+          for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
         }
 
         // ---- joining steps: first minimum magnitude over the 2K candidates.
-        // A candidate is a fraction num/den with den > 0; fractions are
-        // compared by cross-multiplication (no division), in four independent
-        // chains (one per row offset e) to keep the comparisons off one long
-        // dependency chain.  Each lane's winner is then divided exactly and
-        // the warp reduces the exact (|value|, index) pairs: ties go to the
-        // first index as in cblas_iamin.  Infinite candidates (active atoms,
-        // |A_j| beyond the bounds) never decide a step (the step is then
-        // step_max or step_max2).
+        // Row r offers (C + c_r)/(1 + a_r) (index r) and (C - c_r)/(1 - a_r)
+        // (index r + K); with both denominators positive the first is the
+        // smaller one exactly when c_r <= C a_r (ties go to index r), so each
+        // row submits one candidate, or its other one when the first has no
+        // positive denominator (pos submits only the second).  Candidates
+        // are fractions num/den, den > 0, compared by cross-multiplication in
+        // four independent chains (one per row offset e); each lane's winner
+        // is divided exactly and the warp reduces the exact (|value|, index)
+        // pairs, ties to the first index as in cblas_iamin.  Infinite
+        // candidates (active or padding atoms, |A_j| beyond the bounds) never
+        // decide a step (the step is then step_max or step_max2).
         T cn[4], cd[4];
         int ci[4];
 #pragma unroll
@@ -240,19 +239,19 @@ lars_kernel(const LarsArgs<T> a) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int r = r0 + e;
-            const bool active = (act >> (v * 4 + e)) & 1u;
-            const T aa = A[v][e];
-            const bool ok = !active && aa < INF;  // padding rows are marked active
-            if (ok && !pos && aa > T(-1)) {
-              const T num = d.v[e] + C, den = T(1) + aa;
-              const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
-              if (lhs < rhs || (lhs == rhs && r < ci[e])) { cn[e] = num; cd[e] = den; ci[e] = r; }
-            }
-            if (ok && aa < T(1)) {
-              const T num = C - d.v[e], den = T(1) - aa;
-              const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
-              if (lhs < rhs || (lhs == rhs && r + K < ci[e])) { cn[e] = num; cd[e] = den; ci[e] = r + K; }
-            }
+            const bool active = (act >> (v * 4 + e)) & 1u;  // padding rows are marked active
+            const T aa = A[v][e], c = d.v[e];
+            const bool okp = !pos && aa > T(-1) && aa < INF;  // (C + c)/(1 + a) admissible
+            const bool okm = aa < T(1);                       // (C - c)/(1 - a) admissible
+            const bool plus = okp && (!okm || c <= C * aa);
+            const T num = plus ? C + c : C - c;
+            const T den = plus ? T(1) + aa : T(1) - aa;
+            const int idx = plus ? r : r + K;
+            const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
+            const bool take = !active && (okp || okm) && (lhs < rhs || (lhs == rhs && idx < ci[e]));
+            cn[e] = take ? num : cn[e];
+            cd[e] = take ? den : cd[e];
+            ci[e] = take ? idx : ci[e];
           }
         }
 #pragma unroll
