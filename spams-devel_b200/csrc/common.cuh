@@ -80,6 +80,71 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// Order-preserving map of a float to an unsigned key: a < b (as floats, no
+// NaN) exactly when key(a) < key(b) (as unsigned).
+__device__ __forceinline__ unsigned float_key(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// Warp-uniform results of the arg-reductions below (every lane gets them).
+template <typename T> struct ArgRes { T val; int idx; };
+
+// (min key, first index among the minima, the value carried by that entry)
+// over the warp; keys must be non-NaN.  Single precision uses the warp
+// reduction instructions on order-preserving key bits; double precision a
+// butterfly of shuffles.
+__device__ __forceinline__ ArgRes<float> warp_argmin_first(float key, int idx, float carry) {
+  const unsigned kb = float_key(key);
+  const unsigned mn = __reduce_min_sync(kFull, kb);
+  const int wi = (int)__reduce_min_sync(kFull, kb == mn ? (unsigned)idx : 0xffffffffu);
+  const unsigned who = __ballot_sync(kFull, kb == mn && idx == wi);
+  const float v = __shfl_sync(kFull, carry, __ffs(who) - 1);
+  return ArgRes<float>{v, wi};
+}
+__device__ __forceinline__ ArgRes<double> warp_argmin_first(double key, int idx, double carry) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double k2 = __shfl_xor_sync(kFull, key, o);
+    const int i2 = __shfl_xor_sync(kFull, idx, o);
+    const double c2 = __shfl_xor_sync(kFull, carry, o);
+    if (k2 < key || (k2 == key && i2 < idx)) { key = k2; idx = i2; carry = c2; }
+  }
+  return ArgRes<double>{__shfl_sync(kFull, carry, 0), __shfl_sync(kFull, idx, 0)};
+}
+// (min key, LAST index among the minima); idx -1 marks "no candidate".
+__device__ __forceinline__ ArgRes<float> warp_argmin_last_u(float key, int idx) {
+  const unsigned kb = float_key(key);
+  const unsigned mn = __reduce_min_sync(kFull, kb);
+  const int wi = __reduce_max_sync(kFull, kb == mn ? idx : -1);
+  const float v = __shfl_sync(kFull, key, __ffs(__ballot_sync(kFull, kb == mn)) - 1);
+  return ArgRes<float>{v, wi};
+}
+__device__ __forceinline__ ArgRes<double> warp_argmin_last_u(double key, int idx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double k2 = __shfl_xor_sync(kFull, key, o);
+    const int i2 = __shfl_xor_sync(kFull, idx, o);
+    if (k2 < key || (k2 == key && i2 > idx)) { key = k2; idx = i2; }
+  }
+  return ArgRes<double>{__shfl_sync(kFull, key, 0), __shfl_sync(kFull, idx, 0)};
+}
+// (max key, first index among the maxima).
+__device__ __forceinline__ int warp_argmax_first(float key, int idx) {
+  const unsigned kb = float_key(key);
+  const unsigned mx = __reduce_max_sync(kFull, kb);
+  return (int)__reduce_min_sync(kFull, kb == mx ? (unsigned)idx : 0xffffffffu);
+}
+__device__ __forceinline__ int warp_argmax_first(double key, int idx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double k2 = __shfl_xor_sync(kFull, key, o);
+    const int i2 = __shfl_xor_sync(kFull, idx, o);
+    if (k2 > key || (k2 == key && i2 < idx)) { key = k2; idx = i2; }
+  }
+  return __shfl_sync(kFull, idx, 0);
+}
+
 // Arg-min of (key, idx) pairs, ties resolved to the smaller idx.  Keys are
 // compared as given (callers pass magnitudes); NaN keys never win.
 template <typename T>

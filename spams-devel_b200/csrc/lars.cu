@@ -119,8 +119,7 @@ lars_kernel(const LarsArgs<T> a) {
         }
       }
     }
-    warp_argmax(bkey, bidx);
-    int cur = __shfl_sync(kFull, bidx, 0);
+    int cur = warp_argmax_first(bkey, bidx);
     T normX = a.norms[sig];
     for (int j = lane; j < Lc; j += 32) sCoef[j] = 0;  // coeffs.setZeros()
     __syncwarp();
@@ -194,10 +193,9 @@ lars_kernel(const LarsArgs<T> a) {
           const T ratio = -sCoef[r] / s;
           if (ratio > 0 && ratio <= zkey) { zkey = ratio; zidx = r; }
         }
-        warp_argmin_last(zkey, zidx);
-        // lane 0's result drives the (warp-uniform) control flow
-        const T step_max = __shfl_sync(kFull, zkey, 0);
-        const int first_zero = __shfl_sync(kFull, zidx, 0);
+        const ArgRes<T> zr = warp_argmin_last_u(zkey, zidx);  // warp-uniform
+        const T step_max = zr.val;
+        const int first_zero = zr.idx;
         __syncwarp();
         const T C = fabs(sCA[0]);
         c_end = C;
@@ -268,15 +266,9 @@ lars_kernel(const LarsArgs<T> a) {
         T mval = cn[0] / cd[0];
         T mkey = fabs(mval);
         if (!(mkey < INF)) { mkey = INF; mval = INF; }  // NaN never wins
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          const T k2 = __shfl_xor_sync(kFull, mkey, o);
-          const int i2 = __shfl_xor_sync(kFull, midx, o);
-          const T v2 = __shfl_xor_sync(kFull, mval, o);
-          if (k2 < mkey || (k2 == mkey && i2 < midx)) { mkey = k2; midx = i2; mval = v2; }
-        }
-        T step = __shfl_sync(kFull, mval, 0);
-        cur = __shfl_sync(kFull, midx, 0) % K;
+        const ArgRes<T> mr = warp_argmin_first(mkey, midx, mval);  // warp-uniform
+        T step = mr.val;
+        cur = mr.idx % K;
 
         // ---- polynomial of normX along the step
         T p1 = 0, p2 = 0;

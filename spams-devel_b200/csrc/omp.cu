@@ -79,8 +79,7 @@ omp_kernel(const OmpArgs<T> a) {
         }
       }
     }
-    warp_argmax(bkey, bidx);
-    int c = __shfl_sync(kFull, bidx, 0);
+    int c = warp_argmax_first(bkey, bidx);
     __syncwarp();
 
     int j = 0;
@@ -184,8 +183,7 @@ omp_kernel(const OmpArgs<T> a) {
             }
         bkey = ck[0];
         bidx = cix[0];
-        warp_argmax(bkey, bidx);
-        c = __shfl_sync(kFull, bidx, 0);
+        c = warp_argmax_first(bkey, bidx);
         __syncwarp();
       }
     }
