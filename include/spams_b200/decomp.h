@@ -38,13 +38,15 @@ inline sc_status call_omp(const double* X, int m, int64_t n, const double* D, in
 }
 inline sc_status call_lasso(const float* X, int m, int64_t n, const float* D, int K, int L,
                             float l1, float l2, int mode, int pos, int mlp, float* path,
-                            sc_csc_f32* out) {
-  return sc_lasso_f32(X, m, n, D, K, L, l1, l2, mode, pos, 0, -1, mlp, 0, path, nullptr, out);
+                            sc_csc_f32* out, int ols = 0, int cholesky = 0) {
+  return sc_lasso_f32(X, m, n, D, K, L, l1, l2, mode, pos, ols, -1, mlp, cholesky, path, nullptr,
+                      out);
 }
 inline sc_status call_lasso(const double* X, int m, int64_t n, const double* D, int K, int L,
                             double l1, double l2, int mode, int pos, int mlp, double* path,
-                            sc_csc_f64* out) {
-  return sc_lasso_f64(X, m, n, D, K, L, l1, l2, mode, pos, 0, -1, mlp, 0, path, nullptr, out);
+                            sc_csc_f64* out, int ols = 0, int cholesky = 0) {
+  return sc_lasso_f64(X, m, n, D, K, L, l1, l2, mode, pos, ols, -1, mlp, cholesky, path, nullptr,
+                      out);
 }
 inline sc_status call_lassoQq(const float* X, int m, int64_t n, const float* Q, int K,
                               const float* q, int L, float l1, float l2, int mode, int pos,
@@ -155,15 +157,29 @@ void lasso2(const Matrix<T>& X, const Matrix<T>& G, const Matrix<T>& DtX, SpMatr
 }
 
 // decomp/decomp.h:735-841: the Cholesky implementation of the same homotopy.
-// Without ols it follows the same path as lasso2 and is served by it; the ols
-// re-projection is not available and throws.
+// In PENALTY and L1COEFFS modes it follows lasso2's path; ols adds the final
+// least-squares fit on the support.  Its L2ERROR rule is not available
+// (the call throws the engine's message).
 template <typename T>
 void lasso(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha, int L,
            const T constraint, const T lambda2 = 0, constraint_type mode = PENALTY,
            const bool pos = false, const bool ols = false, const int numThreads = -1,
            Matrix<T>* path = NULL, const int length_path = -1) {
-  if (ols) throw "lasso : the ols option is not available in spams_b200";
-  lasso2(X, D, spalpha, L, constraint, lambda2, mode, pos, numThreads, path, length_path);
+  (void)numThreads;
+  namespace d = spams_b200_detail;
+  const INTM n = X.n(), K = D.n();
+  const int Lc = std::min<int>(L, (int)K);
+  const int mlp = length_path <= 1 ? 4 * Lc : length_path;
+  std::vector<T> pbuf(path ? (size_t)K * mlp : 0);
+  typename d::Csc<T>::type out;
+  d::check(d::call_lasso(X.X(), (int)X.m(), n, D.X(), (int)K, L, constraint, lambda2, (int)mode,
+                         pos ? 1 : 0, mlp, path ? pbuf.data() : nullptr, &out, ols ? 1 : 0, 1));
+  d::adopt<T>(out, spalpha);
+  if (path) {
+    const size_t cols = std::min<size_t>((size_t)path->n(), (size_t)mlp);
+    for (size_t c = 0; c < cols; ++c)
+      memcpy(path->rawX() + c * path->m(), pbuf.data() + c * K, sizeof(T) * std::min<INTM>(K, path->m()));
+  }
 }
 
 #endif  // SPAMS_B200_DECOMP_H

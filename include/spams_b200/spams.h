@@ -19,8 +19,6 @@ SpMatrix<T>* _lassoD(Matrix<T>* X, Matrix<T>* D, Matrix<T>** path, bool return_r
   (void)verbose;
   namespace d = spams_b200_detail;
   if (X->m() != D->m()) throw "lasso : incompatible matrix dimensions";
-  if (ols) throw "lasso : the ols option is not available in spams_b200";
-  (void)cholevsky;  // the Cholesky variant follows the same homotopy path
   const int K = (int)D->n();
   const int L0 = L < 0 ? K : L;
   const int mlp = max_length_path < 0 ? 4 * L0 : max_length_path;
@@ -30,7 +28,8 @@ SpMatrix<T>* _lassoD(Matrix<T>* X, Matrix<T>* D, Matrix<T>** path, bool return_r
   typename d::Csc<T>::type out;
   sc_status st = d::call_lasso(X->X(), (int)X->m(), X->n(), D->X(), K, L, constraint, lambda2,
                                (int)mode, pos ? 1 : 0, max_length_path,
-                               *path ? (*path)->rawX() : nullptr, &out);
+                               *path ? (*path)->rawX() : nullptr, &out, ols ? 1 : 0,
+                               (cholevsky || ols) ? 1 : 0);
   if (st != SC_OK) {
     delete alpha;
     delete *path;
@@ -52,7 +51,7 @@ SpMatrix<T>* _lassoQq(Matrix<T>* X, Matrix<T>* Q, Matrix<T>* q, Matrix<T>** path
   namespace d = spams_b200_detail;
   if (Q->m() != Q->n()) throw "lasso : Q must be square";
   if (Q->m() != q->m() || X->n() != q->n()) throw "lasso : incompatible matrix dimensions";
-  if (ols) throw "lasso : the ols option is not available in spams_b200";
+  if (ols) throw "lasso : ols with precomputed (Q, q) is not available in spams_b200";
   const int K = (int)Q->m();
   const int L0 = L < 0 ? K : L;
   const int mlp = max_length_path < 0 ? 4 * L0 : max_length_path;

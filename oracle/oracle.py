@@ -201,8 +201,21 @@ def orc_omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False):
 
 
 def orc_lasso(X, D, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, max_length_path=-1,
-              return_reg_path=False):
-    """C restatement of _lassoD / lasso2 / coreLARS2."""
+              return_reg_path=False, ols=False, cholesky=False):
+    """C restatement of _lassoD / lasso2 / coreLARS2.
+
+    cholesky / ols select the reference's Cholesky implementation (lasso<T>,
+    coreLARS, decomp/decomp.h:735-1093), which follows the same path in PENALTY
+    and L1COEFFS modes; ols then refits the support by least squares
+    (decomp/decomp.h:1087-1091), done here in numpy.  Its L2ERROR rule differs
+    and is not restated."""
+    if (ols or cholesky) and mode == 1:
+        raise NotImplementedError("the Cholesky variant's L2ERROR rule is not restated")
+    if ols:
+        res = orc_lasso(X, D, L, lambda1, lambda2, mode, pos, max_length_path, return_reg_path)
+        a = res[0] if return_reg_path else res
+        a = ols_refit(a, X, D, max(float(lambda2), 1e-10))
+        return (a, res[1]) if return_reg_path else a
     dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
     X, D = _f(X, dt), _f(D, dt)
     m, n = X.shape
@@ -224,3 +237,19 @@ def orc_lasso(X, D, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, max_lengt
        C.c_int(mode), C.c_int(int(pos)), C.c_int(mlp.value), _p(vM), _p(rM), _p(path))
     a = _convert(vM, rM, Lc, n, K, dt)
     return (a, path) if return_reg_path else a
+
+
+def ols_refit(A, X, D, ridge):
+    """Least-squares fit of every column of X on its support in A, with the
+    Gram matrix G = D^T D + ridge I in the precision of X (the ols projection
+    of coreLARS, decomp/decomp.h:1087-1091)."""
+    A = A.tocsc().copy()
+    dt = A.dtype
+    Xd, Dd = np.asarray(X, dtype=np.float64), np.asarray(D, dtype=np.float64)
+    G = Dd.T @ Dd + ridge * np.eye(Dd.shape[1])
+    for j in range(A.shape[1]):
+        s, e = A.indptr[j], A.indptr[j + 1]
+        if e > s:
+            idx = A.indices[s:e]
+            A.data[s:e] = np.linalg.solve(G[np.ix_(idx, idx)], Dd[:, idx].T @ Xd[:, j]).astype(dt)
+    return A

@@ -127,6 +127,8 @@ void release_all() {
 enum : size_t {
   MISC_COUNTERS = 0,     // unsigned[2]: work-queue heads (main pass, overflow pass)
   MISC_OVF_COUNT = 16,   // int: signals sent to the overflow pass
+  MISC_RF_COUNT = 64,    // int: active sets queued to the large-set refinement pass
+  MISC_RF_CTR = 68,      // unsigned: its work-queue head
   MISC_CAPFLAG = 128,    // int: device CSC arrays too small
   MISC_TC_ERR = 192,     // int: tensor-core pipeline wait gave up
   MISC_STEPS = 224,      // unsigned long long: coding steps (profile)
@@ -183,6 +185,9 @@ struct Prof {
 
 static void prof_reset() { memset(&g_prof, 0, sizeof(g_prof)); }
 
+// Blocks of the refinement pass for active sets beyond 32 atoms.
+constexpr int kRefineBigGrid = 32;
+
 // ---------------------------------------------------------------------------
 // launch shapes
 struct Shape {
@@ -231,6 +236,7 @@ struct Problem {
   // BF16 hi/lo tensor-core correlations + FP64 refinement (float only)
   bool tc = false;
   bool refine = false;            // FP64 refinement of the final coefficients
+  bool ols = false;               // least-squares refit on the final support (lasso ols)
   const void* dDsplit = nullptr;  // Dhi (mp x K bf16) followed by Dlo
   int mp = 0;                     // m rounded up to the 64-element k-block
   int* d_tc_err = nullptr;
@@ -266,6 +272,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   const int64_t scan_len = scan_scratch_len(nc);
   SC_TRY(c.scan.reserve((size_t)scan_len * 8));
   if (p.hX) SC_TRY(c.xstage.reserve((size_t)nc * p.m * sizeof(T)));
+  if (p.ols || p.refine) {
+    SC_TRY(c.rlist.reserve((size_t)nc * 8));
+    if (p.L > 32) SC_TRY(c.rscratch.reserve(refine_scratch_bytes(p.L, kRefineBigGrid)));
+  }
   if (p.tc) SC_TRY(c.xsplit.reserve((size_t)nc * p.mp * 4));
   SC_TRY(c.level.reserve((size_t)nc * sizeof(T)));
   if (sink) {
@@ -342,7 +352,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
       a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
       a.gstate = nullptr; a.path = path; a.steps = d_steps;
-      a.out_level = p.refine ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
+      a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
       SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
       pr.launches(1);
       if (may_overflow) {
@@ -373,14 +383,20 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
       }
     }
-    if (p.refine && p.dD) {
-      if constexpr (std::is_same<T, float>::value) {
-        pr.mark(ST_REFINE);
-        SC_CUDA(launch_refine(p.dD, p.m, xchunk, dG, Kp, sind, sval, p.L, cnt,
-                              p.lars ? reinterpret_cast<const float*>(c.level.ptr) : nullptr, cn,
-                              st));
-        pr.launches(1);
-      }
+    // ---- double-precision solves on the final active sets: the ols
+    // projection, or the refinement of single-precision codes
+    if (p.ols || (p.refine && (p.dD || p.dDtX))) {
+      pr.mark(ST_REFINE);
+      const bool with_level = p.lars && !p.ols;
+      const T* q = p.dDtX ? p.dDtX + (size_t)start * p.K : nullptr;
+      SC_CUDA(launch_refine<T>(q ? nullptr : p.dD, p.m, q ? nullptr : xchunk, q, p.K, dG, Kp, sind,
+                               sval, p.L, cnt,
+                               with_level ? reinterpret_cast<const T*>(c.level.ptr) : nullptr, cn,
+                               reinterpret_cast<int64_t*>(c.rlist.ptr),
+                               misc_at<int>(c.misc, MISC_RF_COUNT),
+                               misc_at<unsigned>(c.misc, MISC_RF_CTR),
+                               reinterpret_cast<double*>(c.rscratch.ptr), kRefineBigGrid, st));
+      pr.launches(2);
     }
     if (pr.on && may_overflow) {
       SC_CUDA(cudaMemcpyAsync(c.pinned_small, d_ovf_count, 4, cudaMemcpyDeviceToHost, st));
@@ -650,8 +666,12 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (mode < 0 || mode > 2)
     return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d not supported by the coding path", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
-  if (ols || cholesky)
-    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky/ols variant (lasso<T>, coreLARS) is not implemented");
+  // The Cholesky implementation (lasso<T> / coreLARS, decomp/decomp.h:735-1093)
+  // follows the same path as lasso2 in PENALTY and L1COEFFS modes; its ols
+  // option ends with the least-squares fit on the final support.  Its L2ERROR
+  // stopping rule differs (no exact stop at the constraint) and is not built.
+  if ((ols || cholesky) && mode == SC_L2ERROR)
+    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky variant's L2ERROR rule is not implemented");
   if (path) memset(path, 0, sizeof(T) * (size_t)K * std::max(0, max_length_path));
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);
@@ -690,6 +710,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   }
   p.hX = X; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
+  p.ols = ols != 0;
   // coreLARS2 replaces a path length <= 1 by 4L (decomp/decomp.h:1722) and
   // writes that many columns; the device buffer covers them, only the
   // caller's max_length_path columns are returned.

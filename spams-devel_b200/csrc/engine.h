@@ -34,11 +34,11 @@ struct DeviceCtx {
   std::mutex mu;
   void* pinned_small = nullptr;  // 4 KiB pinned scratch for small readbacks
   Buf X, D, G, dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, gstate;
-  Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level;
+  Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
   std::vector<Buf*> all_bufs() {
     return {&X, &D, &G, &dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc,
             &scan, &gstate, &ccolptr, &crows, &cvals, &path, &vecs, &xstage, &xsplit,
-            &dsplit, &level};
+            &dsplit, &level, &rlist, &rscratch};
   }
 };
 

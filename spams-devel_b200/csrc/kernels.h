@@ -107,16 +107,21 @@ template <typename T>
 cudaError_t launch_pad_rows(const T* src, int K, int64_t ldsrc, int64_t n, T* dst,
                             int Kp, cudaStream_t st);
 
-// ---- FP64 refinement of the final coefficients ----------------------------
+// ---- double-precision solves on the final active sets ---------------------
 // For every signal with a non-empty active set A (sorted atom indices and
-// coefficients in the slabs) recompute, in double precision,
-//     a_A = G_AA^{-1} (D_A^T x - level * sign(a_A))     (lasso, level per signal)
-//     a_A = G_AA^{-1}  D_A^T x                          (OMP: level == NULL)
-// with D_A^T x from the float32 inputs; active sets beyond 32 atoms keep
-// their values.
-cudaError_t launch_refine(const float* D, int m, const float* X, const float* G, int Kp,
-                          const int* slab_ind, float* slab_val, int L, const int* cnt,
-                          const float* level, int64_t n, cudaStream_t st);
+// coefficients in the slabs):
+//     a_A = G_AA^{-1} (D_A^T x - level * sign(a_A))   (level != NULL: lasso refinement)
+//     a_A = G_AA^{-1}  D_A^T x                        (level == NULL: OMP refinement, ols)
+// in double precision.  D_A^T x comes from D and X, or from Q (the caller's
+// D^T X, ld ldq) when Q is given.  Active sets of more than 32 atoms go to a
+// second pass (big_grid blocks of 4 warps, each warp a slab of
+// L (L + 1) + L doubles in `scratch`, refine_scratch_bytes).
+template <typename T>
+cudaError_t launch_refine(const T* D, int m, const T* X, const T* Q, int ldq, const T* G, int Kp,
+                          const int* slab_ind, T* slab_val, int L, const int* cnt, const T* level,
+                          int64_t n, int64_t* big_list, int* big_count, unsigned* counter,
+                          double* scratch, int big_grid, cudaStream_t st);
+size_t refine_scratch_bytes(int L, int grid);
 
 // ---- CSC assembly ----------------------------------------------------------
 // colptr[i+1] = base + cnt[0] + ... + cnt[i]; with base == NULL the base is 0

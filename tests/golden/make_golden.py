@@ -60,6 +60,9 @@ def cases():
     out.append(dict(name="lasso_enet", algo="lasso", X=X, D=D, kw=dict(lambda1=0.1, lambda2=0.5), path=False))
     out.append(dict(name="lasso_path", algo="lasso", X=X[:, :10], D=D, kw=dict(lambda1=0.05, L=12), path=True))
     out.append(dict(name="lasso_big_lambda", algo="lasso", X=X[:, :30], D=D, kw=dict(lambda1=100.0), path=False))
+    # the Cholesky implementation (lasso / coreLARS) and its ols projection
+    out.append(dict(name="lasso_ols", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.1, ols=True), path=False))
+    out.append(dict(name="lasso_chol_l1", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=1.0, mode=0, cholesky=True), path=False))
     # Gaussian signals, LARS runs long with drops (dense active sets, small lambda)
     r = rng(6)
     D = W.gaussian_dictionary(24, 70, r)
