@@ -180,4 +180,18 @@ __device__ __forceinline__ void warp_argmin_last(T& key, int& idx) {
   }
 }
 
+// Persistent-grid size for a kernel whose blocks loop over a work counter:
+// grid > 0 is kept; otherwise as many blocks as fit on the device at once.
+template <typename Kern>
+inline cudaError_t fill_grid(Kern k, int threads, size_t smem, int* grid) {
+  if (*grid > 0) return cudaSuccess;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+  if (e != cudaSuccess) return e;
+  *grid = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  return cudaSuccess;
+}
+
 }  // namespace sc

@@ -187,18 +187,38 @@ static void prof_reset() { memset(&g_prof, 0, sizeof(g_prof)); }
 
 // Blocks of the refinement pass for active sets beyond 32 atoms.
 constexpr int kRefineBigGrid = 32;
+// Largest padded atom count of the warp-per-signal kernels, and of the
+// CTA-per-signal ones.
+constexpr int kWarpMaxKp = 1024;
+constexpr int kCtaMaxKp = 4096;
 
 // ---------------------------------------------------------------------------
 // launch shapes
 struct Shape {
+  bool cta;   // one CTA per signal (Kp > kWarpMaxKp)
   int Lcap;   // active-set capacity in shared memory
-  int wpb;    // warps per block
-  int grid;   // persistent blocks
+  int wpb;    // warps per block (warp kernels)
+  int grid;   // persistent blocks (0: filled by the CTA launcher)
 };
 
 template <typename T>
 static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
   Shape s;
+  s.cta = Kp > kWarpMaxKp;
+  if (s.cta) {
+    // the small state is per CTA, so it can hold more atoms; keep two CTAs
+    // per SM within the shared-memory budget
+    s.wpb = Kp / 512;
+    s.grid = 0;
+    auto bytes = [&](int lc) {
+      return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
+    };
+    s.Lcap = std::max(1, std::min(L, 80));
+    while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
+                           2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
+      s.Lcap -= 16;
+    return s;
+  }
   s.Lcap = std::max(1, std::min(L, 32));
   s.wpb = 8;
   const size_t per_warp = lars ? lars_state_bytes(Kp, s.Lcap, sizeof(T))
@@ -284,11 +304,13 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_TRY(c.cvals.reserve((size_t)nc * p.L * sizeof(T)));
     sink->colptr.assign((size_t)p.n + 1, 0);
   }
-  // overflow pass: state in global slabs with capacity L
-  const int ovf_wpb = 4;
-  const size_t ovf_per_warp = p.lars ? lars_state_bytes(Kp, p.L, sizeof(T))
-                                     : omp_state_bytes(Kp, p.L, sizeof(T));
-  int ovf_grid = c.num_sms;
+  // overflow pass: state in global slabs with capacity L (per warp, or per
+  // CTA for the CTA-per-signal kernels)
+  const int ovf_wpb = shp.cta ? 1 : 4;
+  const size_t ovf_per_warp =
+      shp.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
+              : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
+  int ovf_grid = shp.cta ? 2 * c.num_sms : c.num_sms;
   while (ovf_grid > 1 && (size_t)ovf_grid * ovf_wpb * ovf_per_warp > ((size_t)256 << 20))
     ovf_grid >>= 1;
   const bool may_overflow = shp.Lcap < p.L;
@@ -353,14 +375,16 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
       a.gstate = nullptr; a.path = path; a.steps = d_steps;
       a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
-      SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
+      if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
+      else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
       pr.launches(1);
       if (may_overflow) {
         pr.launches(1);
         a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
         a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
         a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
-        SC_CUDA(launch_lars<T>(a, ovf_grid, ovf_wpb, st));
+        if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ovf_grid, st));
+        else SC_CUDA(launch_lars<T>(a, ovf_grid, ovf_wpb, st));
       }
     } else {
       OmpArgs<T> a{};
@@ -373,14 +397,16 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
       a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
       a.path = path; a.steps = d_steps;
-      SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
+      if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, shp.grid, st));
+      else SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
       pr.launches(1);
       if (may_overflow) {
         pr.launches(1);
         a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
         a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
         a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
-        SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
+        if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, ovf_grid, st));
+        else SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
       }
     }
     // ---- double-precision solves on the final active sets: the ols
@@ -480,6 +506,12 @@ static sc_status emit_sink(int64_t m, int64_t n, HostSink<T>& s, typename CscOf<
 }
 
 static inline int pad128(int K) { return ((K + 127) / 128) * 128; }
+// Padded atom count: a multiple of 128 up to 1024 atoms (one warp per signal),
+// of 512 beyond (one CTA of Kp / 512 warps per signal).
+static inline int pad_atoms(int K) {
+  const int p = pad128(K);
+  return p <= kWarpMaxKp ? p : ((K + 511) / 512) * 512;
+}
 
 // Per-call device guard: serialises calls on one device and orders this
 // call's stream after the previous user of the shared workspaces.
@@ -538,8 +570,9 @@ static sc_status check_tc(DeviceCtx& c, cudaStream_t st, const Problem<T>& p) {
 }
 
 static sc_status check_kp(int K) {
-  if (pad128(K) > 1024)
-    return fail(SC_ERR_UNSUPPORTED, "dictionaries with more than 1024 atoms are not supported yet (K=%d)", K);
+  if (pad_atoms(K) > kCtaMaxKp)
+    return fail(SC_ERR_UNSUPPORTED, "dictionaries with more than %d atoms are not supported (K=%d)",
+                kCtaMaxKp, K);
   return SC_OK;
 }
 
@@ -585,7 +618,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  const int Kp = pad128(K);
+  const int Kp = pad_atoms(K);
   SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -685,7 +718,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  const int Kp = pad128(K);
+  const int Kp = pad_atoms(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   Problem<T> p;
   p.lars = true;
@@ -777,7 +810,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
     SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
     return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
   }
-  const int Kp = pad128(K);
+  const int Kp = pad_atoms(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
   pr.mark(ST_GRAM);
@@ -820,7 +853,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
     SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
     return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
   }
-  const int Kp = pad128(K);
+  const int Kp = pad_atoms(K);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   pr.mark(ST_GRAM);
   SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));

@@ -84,8 +84,24 @@ cudaError_t launch_lars(const LarsArgs<T>& a, int grid, int warps_per_block, cud
 template <typename T>
 int lars_max_warps_per_sm(int Kp);
 
+// One CTA of Kp / 512 warps per signal (Kp a multiple of 512, 1024..4096);
+// a.gstate set: per-CTA small state in global slabs (lars_cta_gstate_bytes).
+// grid <= 0: as many persistent blocks as fit on the device.
+template <typename T>
+cudaError_t launch_lars_cta(const LarsArgs<T>& a, int grid, cudaStream_t st);
+template <typename T>
+size_t lars_cta_smem_bytes(int Kp, int Lc, bool gstate);
+template <typename T>
+size_t lars_cta_gstate_bytes(int Lc, int grid);
+
 template <typename T>
 cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);
+template <typename T>
+cudaError_t launch_omp_cta(const OmpArgs<T>& a, int grid, cudaStream_t st);
+template <typename T>
+size_t omp_cta_smem_bytes(int Kp, int Lc, bool gstate);
+template <typename T>
+size_t omp_cta_gstate_bytes(int Lc, int grid);
 template <typename T>
 int omp_max_warps_per_sm(int Kp);
 

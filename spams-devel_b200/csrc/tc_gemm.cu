@@ -323,8 +323,14 @@ cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* 
   if (n <= 0 || K <= 0) return cudaSuccess;
   if (!load_encode()) return cudaErrorNotSupported;
   const int Kp = ((K + TC_BM - 1) / TC_BM) * TC_BM;
-  if (m_pad % TC_BK != 0 || nterms < 1 || nterms > 3 || rows_out > Kp || ldc < rows_out)
+  if (m_pad % TC_BK != 0 || nterms < 1 || nterms > 3 || ldc < rows_out)
     return cudaErrorInvalidValue;
+  if (rows_out > Kp) {  // rows past the last tile (a wider padding of K) are zero
+    cudaError_t e = cudaMemset2DAsync(C + Kp, (size_t)ldc * sizeof(float), 0,
+                                      (size_t)(rows_out - Kp) * sizeof(float), (size_t)n, st);
+    if (e != cudaSuccess) return e;
+    rows_out = Kp;
+  }
   CUtensorMap mAh, mAl, mBh, mBl;
   if (!make_map(&mAh, Dhi, m_pad, K, TC_BM) || !make_map(&mAl, Dlo, m_pad, K, TC_BM) ||
       !make_map(&mBh, Xhi, m_pad, n, TC_BN) || !make_map(&mBl, Xlo, m_pad, n, TC_BN))

@@ -120,14 +120,16 @@ REF_FLOAT_DIVERGES = {"lasso_ols"}
 
 def objective(g, A, dt=np.float64):
     """Per-column objective of the case: lasso 0.5||x-Da||^2 + lambda||a||_1
-    (mode 2), the residual ||x - Da||^2 otherwise."""
+    (mode 2 without ols), the residual ||x - Da||^2 otherwise (OMP, the
+    constrained modes, and the ols projection, which minimises the residual
+    on its support)."""
     X = g["X"].astype(np.float64)
     D = g["D"].astype(np.float64)
     A = A.tocsc().astype(np.float64)
     R = X - (A.T @ D.T).T
     r2 = (R * R).sum(axis=0)
     lam = float(g["kw"].get("lambda1", 0.0))
-    if g["algo"] != "omp" and int(g["kw"].get("mode", 2)) == 2:
+    if g["algo"] != "omp" and int(g["kw"].get("mode", 2)) == 2 and not bool(g["kw"].get("ols", False)):
         l1 = np.asarray(abs(A).sum(axis=0)).ravel()
         return 0.5 * r2 + lam * l1
     return r2
