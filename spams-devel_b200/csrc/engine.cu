@@ -75,6 +75,22 @@ void Buf::release() {
   bytes = 0;
 }
 
+sc_status DeviceCtx::pinned_cols(size_t bytes) {
+  if (bytes <= pinned_col_bytes) return SC_OK;
+  if (pinned_col) cudaFreeHost(pinned_col);
+  pinned_col = nullptr;
+  pinned_col_bytes = 0;
+  cudaError_t e = cudaHostAlloc(&pinned_col, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    pinned_col = nullptr;
+    cudaGetLastError();
+    return fail(SC_ERR_OUT_OF_MEMORY, "cudaHostAlloc(%zu bytes) failed: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  pinned_col_bytes = bytes;
+  return SC_OK;
+}
+
 static std::mutex g_ctx_mu;
 static std::vector<DeviceCtx*> g_ctx;
 
@@ -100,6 +116,14 @@ sc_status get_ctx(int device, DeviceCtx** out) {
     SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
     SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     SC_CUDA(cudaHostAlloc(&c->pinned_small, 4096, cudaHostAllocDefault));
+    SC_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+    SC_CUDA(cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      SC_CUDA(cudaEventCreateWithFlags(&c->ev_h2d[i], cudaEventDisableTiming));
+      SC_CUDA(cudaEventCreateWithFlags(&c->ev_xfree[i], cudaEventDisableTiming));
+      SC_CUDA(cudaEventCreateWithFlags(&c->ev_out[i], cudaEventDisableTiming));
+      SC_CUDA(cudaEventCreateWithFlags(&c->ev_d2h[i], cudaEventDisableTiming));
+    }
     g_ctx[device] = c;
   }
   *out = g_ctx[device];
@@ -116,6 +140,12 @@ void release_all() {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->last_use) cudaEventDestroy(c->last_use);
     if (c->pinned_small) cudaFreeHost(c->pinned_small);
+    if (c->pinned_col) cudaFreeHost(c->pinned_col);
+    for (cudaStream_t s : {c->h2d_stream, c->d2h_stream})
+      if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    for (int i = 0; i < 2; ++i)
+      for (cudaEvent_t e : {c->ev_h2d[i], c->ev_xfree[i], c->ev_out[i], c->ev_d2h[i]})
+        if (e) cudaEventDestroy(e);
     delete c;
     c = nullptr;
   }
@@ -262,25 +292,62 @@ struct Problem {
   int* d_tc_err = nullptr;
 };
 
+// CSC result assembled on the host: malloc'd arrays whose ownership moves to
+// the caller's sc_csc_* (freed by sc_csc_free_*).
 template <typename T>
 struct HostSink {
-  std::vector<int64_t> colptr;
-  std::vector<int32_t> rows;
-  std::vector<T> vals;
+  int64_t* colptr = nullptr;
+  int32_t* rows = nullptr;
+  T* vals = nullptr;
+  size_t cap = 0, nnz = 0;
+  HostSink() = default;
+  HostSink(const HostSink&) = delete;
+  HostSink& operator=(const HostSink&) = delete;
+  ~HostSink() { free(colptr); free(rows); free(vals); }
+  sc_status init(int64_t n) {
+    colptr = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+    if (!colptr) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+    return SC_OK;
+  }
+  sc_status grow(size_t need) {
+    if (need <= cap) return SC_OK;
+    size_t c2 = std::max(need, cap + cap / 2);
+    int32_t* r = (int32_t*)realloc(rows, c2 * sizeof(int32_t));
+    if (!r) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+    rows = r;
+    T* v = (T*)realloc(vals, c2 * sizeof(T));
+    if (!v) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+    vals = v;
+    cap = c2;
+    return SC_OK;
+  }
 };
+
+// Host-array calls code their signals in chunks of about n / kPipeChunks
+// (at least kPipeMinChunk signals): while one chunk is coded, the next one is
+// copied in on the H2D stream and the previous chunk's CSC is read back.
+constexpr int kPipeChunks = 6;
+constexpr int64_t kPipeMinChunk = 16384;
 
 template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
   const Shape shp = pick_shape<T>(c, p.lars, Kp, p.L);
+  const bool piped = sink && p.hX;
+  const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
   const size_t per_sig = (size_t)Kp * sizeof(T) + (size_t)p.L * (sizeof(T) + 4) + 64 +
-                         (p.hX ? (size_t)p.m * sizeof(T) : 0) + (p.tc ? (size_t)p.mp * 4 : 0) +
-                         (sink ? (size_t)p.L * (sizeof(T) + 4) + 8 : 0);
+                         (p.hX ? (size_t)nbuf * p.m * sizeof(T) : 0) +
+                         (p.tc ? (size_t)p.mp * 4 : 0) +
+                         (sink ? (size_t)nbuf * (p.L * (sizeof(T) + 4) + 8) : 0);
   int64_t nc = (int64_t)std::max<size_t>(4096, ((size_t)2 << 30) / per_sig);
   nc = std::min<int64_t>(nc, std::max<int64_t>(p.n, 1));
   nc = std::min<int64_t>(nc, (int64_t)1 << 30);
+  if (piped) {
+    const int64_t k = std::max<int64_t>(1, std::min<int64_t>(kPipeChunks, p.n / kPipeMinChunk));
+    nc = std::min<int64_t>(nc, (p.n + k - 1) / k);
+  }
 
   SC_TRY(c.dtx.reserve((size_t)Kp * nc * sizeof(T)));
   SC_TRY(c.norms.reserve((size_t)nc * sizeof(T)));
@@ -291,18 +358,22 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   SC_TRY(c.misc.reserve(MISC_BYTES));
   const int64_t scan_len = scan_scratch_len(nc);
   SC_TRY(c.scan.reserve((size_t)scan_len * 8));
-  if (p.hX) SC_TRY(c.xstage.reserve((size_t)nc * p.m * sizeof(T)));
+  const size_t xslot = align16((size_t)nc * p.m * sizeof(T));
+  if (p.hX) SC_TRY(c.xstage.reserve(xslot * nbuf));
   if (p.ols || p.refine) {
     SC_TRY(c.rlist.reserve((size_t)nc * 8));
     if (p.L > 32) SC_TRY(c.rscratch.reserve(refine_scratch_bytes(p.L, kRefineBigGrid)));
   }
   if (p.tc) SC_TRY(c.xsplit.reserve((size_t)nc * p.mp * 4));
   SC_TRY(c.level.reserve((size_t)nc * sizeof(T)));
+  const size_t col_slot = align16((size_t)(nc + 1) * 8);
+  const size_t ent_slot = (size_t)nc * p.L;
   if (sink) {
-    SC_TRY(c.ccolptr.reserve((size_t)(nc + 1) * 8));
-    SC_TRY(c.crows.reserve((size_t)nc * p.L * 4));
-    SC_TRY(c.cvals.reserve((size_t)nc * p.L * sizeof(T)));
-    sink->colptr.assign((size_t)p.n + 1, 0);
+    SC_TRY(c.ccolptr.reserve(col_slot * nbuf));
+    SC_TRY(c.crows.reserve(align16(ent_slot * 4) * nbuf));
+    SC_TRY(c.cvals.reserve(align16(ent_slot * sizeof(T)) * nbuf));
+    SC_TRY(c.pinned_cols(col_slot * nbuf));
+    SC_TRY(sink->init(p.n));
   }
   // overflow pass: state in global slabs with capacity L (per warp, or per
   // CTA for the CTA-per-signal kernels)
@@ -323,18 +394,70 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
   g_prof.signals += p.n;
 
+  const int64_t nchunks = p.n > 0 ? (p.n + nc - 1) / nc : 0;
+  auto chunk_len = [&](int64_t i) { return std::min<int64_t>(nc, p.n - i * nc); };
+  auto xslot_ptr = [&](int64_t i) {
+    return reinterpret_cast<T*>(static_cast<char*>(c.xstage.ptr) + (i & 1) * (piped ? xslot : 0));
+  };
+  // copy of chunk i's signals into its staging slot, once the chunk that used
+  // the slot before has finished reading it
+  auto issue_h2d = [&](int64_t i) -> sc_status {
+    cudaStream_t cs = piped ? c.h2d_stream : st;
+    if (piped) SC_CUDA(cudaStreamWaitEvent(cs, c.ev_xfree[i & 1], 0));
+    SC_CUDA(cudaMemcpyAsync(xslot_ptr(i), p.hX + (size_t)(i * nc) * p.m,
+                            (size_t)chunk_len(i) * p.m * sizeof(T), cudaMemcpyHostToDevice, cs));
+    if (piped) SC_CUDA(cudaEventRecord(c.ev_h2d[i & 1], cs));
+    return SC_OK;
+  };
+  // chunk i's CSC: its column pointers were read back into pinned memory on
+  // the coding stream; the entries are copied straight into the result
   int64_t nnz_total = 0;
-  for (int64_t start = 0; start < p.n; start += nc) {
-    const int64_t cn = std::min<int64_t>(nc, p.n - start);
+  auto finalize = [&](int64_t i) -> sc_status {
+    const int64_t cn = chunk_len(i);
+    const int slot = piped ? (int)(i & 1) : 0;
+    SC_CUDA(cudaEventSynchronize(c.ev_out[slot]));
+    const int64_t* hcol =
+        reinterpret_cast<const int64_t*>(static_cast<char*>(c.pinned_col) + slot * col_slot);
+    const int64_t cnnz = hcol[cn];
+    SC_TRY(sink->grow((size_t)(nnz_total + cnnz)));
+    if (cnnz > 0) {
+      cudaStream_t cs = piped ? c.d2h_stream : st;
+      SC_CUDA(cudaMemcpyAsync(sink->rows + nnz_total,
+                              static_cast<char*>(c.crows.ptr) + slot * align16(ent_slot * 4),
+                              (size_t)cnnz * 4, cudaMemcpyDeviceToHost, cs));
+      SC_CUDA(cudaMemcpyAsync(sink->vals + nnz_total,
+                              static_cast<char*>(c.cvals.ptr) + slot * align16(ent_slot * sizeof(T)),
+                              (size_t)cnnz * sizeof(T), cudaMemcpyDeviceToHost, cs));
+      SC_CUDA(cudaEventRecord(c.ev_d2h[slot], cs));
+      SC_CUDA(cudaEventSynchronize(c.ev_d2h[slot]));
+    }
+    int64_t* dst = sink->colptr + i * nc;
+    for (int64_t k = 0; k <= cn; ++k) dst[k] = nnz_total + hcol[k];
+    nnz_total += cnnz;
+    sink->nnz = (size_t)nnz_total;
+    return SC_OK;
+  };
+
+  if (piped && nchunks > 0) {
+    SC_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.last_use, 0));
+    SC_TRY(issue_h2d(0));
+  }
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    const int64_t start = ci * nc;
+    const int64_t cn = chunk_len(ci);
     T* dtx = reinterpret_cast<T*>(c.dtx.ptr);
     T* norms = reinterpret_cast<T*>(c.norms.ptr);
     // ---- inputs: ||x||^2 and D^T x
     const T* xchunk = nullptr;
     pr.mark(ST_OTHER);
     if (p.hX) {
-      SC_CUDA(cudaMemcpyAsync(c.xstage.ptr, p.hX + (size_t)start * p.m,
-                              (size_t)cn * p.m * sizeof(T), cudaMemcpyHostToDevice, st));
-      xchunk = reinterpret_cast<const T*>(c.xstage.ptr);
+      if (piped) {
+        if (ci + 1 < nchunks) SC_TRY(issue_h2d(ci + 1));
+        SC_CUDA(cudaStreamWaitEvent(st, c.ev_h2d[ci & 1], 0));
+      } else {
+        SC_TRY(issue_h2d(ci));
+      }
+      xchunk = xslot_ptr(ci);
     } else {
       xchunk = p.dX + (size_t)start * p.m;
     }
@@ -424,6 +547,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                                reinterpret_cast<double*>(c.rscratch.ptr), kRefineBigGrid, st));
       pr.launches(2);
     }
+    if (piped) SC_CUDA(cudaEventRecord(c.ev_xfree[ci & 1], st));  // staging slot free again
     if (pr.on && may_overflow) {
       SC_CUDA(cudaMemcpyAsync(c.pinned_small, d_ovf_count, 4, cudaMemcpyDeviceToHost, st));
       SC_CUDA(cudaStreamSynchronize(st));
@@ -434,27 +558,22 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     pr.launches(4);
     int64_t* scratch = reinterpret_cast<int64_t*>(c.scan.ptr);
     if (sink) {
-      int64_t* ccol = reinterpret_cast<int64_t*>(c.ccolptr.ptr);
+      const int slot = piped ? (int)(ci & 1) : 0;
+      // the read-back of the chunk that used these slots before has ended
+      // (finalize waits for it on the host)
+      int64_t* ccol = reinterpret_cast<int64_t*>(static_cast<char*>(c.ccolptr.ptr) + slot * col_slot);
+      int32_t* crow = reinterpret_cast<int32_t*>(static_cast<char*>(c.crows.ptr) +
+                                                 slot * align16(ent_slot * 4));
+      T* cval = reinterpret_cast<T*>(static_cast<char*>(c.cvals.ptr) +
+                                     slot * align16(ent_slot * sizeof(T)));
       SC_CUDA(launch_scan_counts(cnt, cn, ccol, nullptr, scratch, scan_len, st));
       SC_CUDA(launch_csc_gather<T>(sind, sval, p.L, cnt, ccol, cn, nullptr, cn * (int64_t)p.L,
-                                   d_capflag, reinterpret_cast<int32_t*>(c.crows.ptr),
-                                   reinterpret_cast<T*>(c.cvals.ptr), st));
-      std::vector<int64_t> hcol((size_t)cn + 1);
-      SC_CUDA(cudaMemcpyAsync(hcol.data(), ccol, (size_t)(cn + 1) * 8, cudaMemcpyDeviceToHost, st));
-      SC_CUDA(cudaStreamSynchronize(st));
-      const int64_t cnnz = hcol[cn];
-      const size_t old = sink->rows.size();
-      sink->rows.resize(old + cnnz);
-      sink->vals.resize(old + cnnz);
-      if (cnnz > 0) {
-        SC_CUDA(cudaMemcpyAsync(sink->rows.data() + old, c.crows.ptr, (size_t)cnnz * 4,
-                                cudaMemcpyDeviceToHost, st));
-        SC_CUDA(cudaMemcpyAsync(sink->vals.data() + old, c.cvals.ptr, (size_t)cnnz * sizeof(T),
-                                cudaMemcpyDeviceToHost, st));
-      }
-      for (int64_t i = 0; i <= cn; ++i) sink->colptr[start + i] = nnz_total + hcol[i];
-      nnz_total += cnnz;
-      SC_CUDA(cudaStreamSynchronize(st));
+                                   d_capflag, crow, cval, st));
+      SC_CUDA(cudaMemcpyAsync(static_cast<char*>(c.pinned_col) + slot * col_slot, ccol,
+                              (size_t)(cn + 1) * 8, cudaMemcpyDeviceToHost, st));
+      SC_CUDA(cudaEventRecord(c.ev_out[slot], st));
+      if (!piped) SC_TRY(finalize(ci));
+      else if (ci >= 1) SC_TRY(finalize(ci - 1));
     } else {
       int64_t* col = p.d_colptr + start;
       SC_CUDA(launch_scan_counts(cnt, cn, col, start == 0 ? nullptr : col, scratch, scan_len, st));
@@ -462,6 +581,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                                    p.d_rows, p.d_vals, st));
     }
   }
+  if (piped && nchunks > 0) SC_TRY(finalize(nchunks - 1));
   pr.mark(ST_OTHER);
   if (d_steps) {
     SC_CUDA(cudaMemcpyAsync(c.pinned_small, d_steps, 8, cudaMemcpyDeviceToHost, st));
@@ -492,16 +612,17 @@ static sc_status emit_empty(int64_t m, int64_t n, typename CscOf<T>::type* out) 
 
 template <typename T>
 static sc_status emit_sink(int64_t m, int64_t n, HostSink<T>& s, typename CscOf<T>::type* out) {
+  if (!s.colptr) SC_TRY(s.init(n));
+  if (!s.rows) SC_TRY(s.grow(1));
   out->m = m;
   out->n = n;
-  out->nnz = s.colptr.empty() ? 0 : s.colptr.back();
-  out->colptr = (int64_t*)malloc(sizeof(int64_t) * ((size_t)n + 1));
-  out->rows = (int32_t*)malloc(sizeof(int32_t) * std::max<size_t>(1, s.rows.size()));
-  out->vals = (T*)malloc(sizeof(T) * std::max<size_t>(1, s.vals.size()));
-  if (!out->colptr || !out->rows || !out->vals) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
-  if (n >= 0) memcpy(out->colptr, s.colptr.data(), sizeof(int64_t) * ((size_t)n + 1));
-  if (!s.rows.empty()) memcpy(out->rows, s.rows.data(), sizeof(int32_t) * s.rows.size());
-  if (!s.vals.empty()) memcpy(out->vals, s.vals.data(), sizeof(T) * s.vals.size());
+  out->nnz = (int64_t)s.nnz;
+  out->colptr = s.colptr;
+  out->rows = s.rows;
+  out->vals = s.vals;
+  s.colptr = nullptr;
+  s.rows = nullptr;
+  s.vals = nullptr;
   return SC_OK;
 }
 

@@ -33,6 +33,13 @@ struct DeviceCtx {
   cudaEvent_t last_use = nullptr;  // end of the previous call's device work
   std::mutex mu;
   void* pinned_small = nullptr;  // 4 KiB pinned scratch for small readbacks
+  // chunk pipeline of the host-array calls: input copies and result
+  // read-backs on their own streams, double-buffered slots
+  cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
+  cudaEvent_t ev_h2d[2] = {}, ev_xfree[2] = {}, ev_out[2] = {}, ev_d2h[2] = {};
+  void* pinned_col = nullptr;  // pinned column pointers of the chunks being read back
+  size_t pinned_col_bytes = 0;
+  sc_status pinned_cols(size_t bytes);
   Buf X, D, G, dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, gstate;
   Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
   std::vector<Buf*> all_bufs() {

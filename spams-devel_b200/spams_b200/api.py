@@ -55,17 +55,52 @@ def _raise(status: int) -> None:
     raise ScError(status, msg)
 
 
+class _EngineCsc:
+    """Owner of an engine-allocated CSC result: numpy arrays viewing its
+    arrays keep it alive, and it is handed back to sc_csc_free_* when the
+    last of them goes away (no copy of the result on the way out)."""
+
+    def __init__(self, out, f64: bool):
+        self.out = out
+        self.f64 = f64
+
+    def view(self, ptr, count: int, typestr: str) -> np.ndarray:
+        holder = _Holder(self, C.cast(ptr, C.c_void_p).value, count, typestr)
+        return np.asarray(holder)
+
+    def __del__(self):
+        try:
+            (_lib.lib().sc_csc_free_f64 if self.f64 else _lib.lib().sc_csc_free_f32)(
+                C.byref(self.out))
+        except Exception:
+            pass
+
+
+class _Holder:
+    def __init__(self, owner: _EngineCsc, addr: int, count: int, typestr: str):
+        self.owner = owner
+        self.__array_interface__ = {"data": (addr, False), "shape": (count,),
+                                    "typestr": typestr, "version": 3}
+
+
 def _csc_from(out, f64: bool) -> ssp.csc_matrix:
     m, n, nnz = int(out.m), int(out.n), int(out.nnz)
-    colptr = np.ctypeslib.as_array(out.colptr, shape=(n + 1,)).copy()
+    own = _EngineCsc(out, f64)
+    colptr = own.view(out.colptr, n + 1, "<i8")
     if nnz > 0:
-        rows = np.ctypeslib.as_array(out.rows, shape=(nnz,)).copy()
-        vals = np.ctypeslib.as_array(out.vals, shape=(nnz,)).copy()
+        rows = own.view(out.rows, nnz, "<i4")
+        vals = own.view(out.vals, nnz, "<f8" if f64 else "<f4")
     else:
         rows = np.zeros(0, np.int32)
         vals = np.zeros(0, np.float64 if f64 else np.float32)
-    (_lib.lib().sc_csc_free_f64 if f64 else _lib.lib().sc_csc_free_f32)(C.byref(out))
-    return ssp.csc_matrix((vals, rows, colptr), shape=(m, n))
+    # one index type for both arrays, as scipy's sparse kernels expect
+    if nnz < 2**31 - 1 and max(m, n) < 2**31 - 1:
+        colptr = colptr.astype(np.int32)
+    else:
+        rows = rows.astype(np.int64)
+    a = ssp.csc_matrix((vals, rows, colptr), shape=(m, n), copy=False)
+    a.has_sorted_indices = True  # rows ascend within every column
+    return a
 
 
 def _vec(v, dtype, n: int):
