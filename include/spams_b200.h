@@ -212,6 +212,72 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
 sc_status sc_corr_bf16x3_noalloc_f32(const float* dD, int m, int K, const float* dX, int64_t n,
                                      float* dC, int ldc, void* stream);
 
+/* ---- Serving: a request loop over resident dictionaries -----------------
+ * No counterpart in the reference (each SPAMS call is synchronous and brings
+ * its own dictionary).  A server keeps dictionaries resident on one GPU (D,
+ * its Gram matrices and BF16 split, keyed by a caller-chosen id) and codes the
+ * requests submitted to it, float32 only.  `slots` worker threads each own a
+ * CUDA stream and workspaces; a free slot takes the oldest pending request and
+ * merges every pending request with the same dictionary and options
+ * (algorithm; Lasso mode, pos and L; precision; refine) into one launch of at
+ * most max_batch_signals signals, with per-signal L / eps / lambda.  A launch
+ * is admitted when the resident dictionaries plus every slot's workspaces stay
+ * within hbm_budget_bytes; a request that cannot fit even alone fails with
+ * SC_ERR_OUT_OF_MEMORY.  Each signal is coded exactly as sc_omp_f32 /
+ * sc_lasso_f32 code it (L, eps, lambda1, mode, pos with their facade
+ * defaults), whichever requests share its launch. */
+typedef struct sc_server sc_server;
+
+enum { SC_REQ_OMP = 0, SC_REQ_LASSO = 1 };
+/* sc_request.flags: the server frees the result itself (replays, load tests). */
+enum { SC_REQ_DISCARD = 1 };
+
+typedef struct {
+  int64_t dict_id;
+  int algo;          /* SC_REQ_OMP or SC_REQ_LASSO */
+  const float* X;    /* host, m x n column-major; valid until the request completes */
+  int64_t n;
+  int L;             /* OMP: <= 0 means not given (min(m, K)); Lasso: as _lassoD (-1: K) */
+  float eps;         /* OMP: residual target (0: not given) */
+  float lambda1;     /* OMP: lambda (0: not given); Lasso: lambda1 */
+  int mode;          /* Lasso: SC_L1COEFFS / SC_L2ERROR / SC_PENALTY */
+  int pos;           /* Lasso: non-negative codes */
+  int precision;     /* SC_PREC_FP32 or SC_PREC_BF16X3 */
+  int refine;        /* FP64 refinement of the final coefficients */
+  int flags;         /* SC_REQ_DISCARD */
+} sc_request;
+
+typedef struct {
+  int64_t completed, signals, batches, rejected, pending;
+  double lat_p50_ms, lat_p99_ms, lat_mean_ms, lat_max_ms; /* arrival to result on the host */
+  double busy_s;                /* wall time with at least one launch in flight */
+  int64_t peak_device_bytes;    /* high-water mark of the admission count */
+  double mean_batch_requests;   /* requests merged per launch */
+} sc_server_stats;
+
+sc_status sc_server_create(int device, int64_t hbm_budget_bytes, int slots,
+                           int64_t max_batch_signals, sc_server** out);
+/* Codes the requests still pending, then frees everything. */
+sc_status sc_server_destroy(sc_server* s);
+/* Uploads D (host, m x K column-major) and forms its Grams (blocking). */
+sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const float* D, int m,
+                                       int K);
+/* Fails while requests against the dictionary are pending or in flight. */
+sc_status sc_server_remove_dictionary(sc_server* s, int64_t dict_id);
+sc_status sc_server_submit(sc_server* s, const sc_request* r, int64_t* ticket);
+/* Blocks until the request is done (or timeout_s passes: SC_ERR_TIMEOUT, the
+ * ticket stays valid); returns its K x n CSC (free with sc_csc_free_f32) and
+ * its latency from submission. */
+sc_status sc_server_wait(sc_server* s, int64_t ticket, double timeout_s, sc_csc_f32* out,
+                         double* latency_ms);
+/* Open-loop load: submits reqs[i] at arrival_s[i] seconds after the call
+ * starts (results discarded; latency counted from the scheduled arrival) and
+ * returns when all have completed. */
+sc_status sc_server_replay(sc_server* s, const sc_request* reqs, const double* arrival_s,
+                           int64_t count);
+/* Counters and latency percentiles since the last reset. */
+sc_status sc_server_stats_get(sc_server* s, int reset, sc_server_stats* out);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

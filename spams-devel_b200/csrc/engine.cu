@@ -35,21 +35,6 @@ sc_status fail(sc_status st, const char* fmt, ...) {
 }
 const char* last_error() { return g_err; }
 
-#define SC_CUDA(call)                                                              \
-  do {                                                                             \
-    cudaError_t _e = (call);                                                       \
-    if (_e != cudaSuccess)                                                         \
-      return fail(_e == cudaErrorMemoryAllocation ? SC_ERR_OUT_OF_MEMORY          \
-                                                  : SC_ERR_CUDA,                   \
-                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
-                  __LINE__);                                                       \
-  } while (0)
-
-#define SC_TRY(expr)                    \
-  do {                                  \
-    sc_status _s = (expr);              \
-    if (_s != SC_OK) return _s;         \
-  } while (0)
 
 // ---------------------------------------------------------------------------
 // device buffers (grow-only, cached per device)
@@ -94,7 +79,7 @@ sc_status DeviceCtx::pinned_cols(size_t bytes) {
 static std::mutex g_ctx_mu;
 static std::vector<DeviceCtx*> g_ctx;
 
-sc_status get_ctx(int device, DeviceCtx** out) {
+static sc_status count_devices(int device) {
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count <= 0) {
@@ -104,12 +89,15 @@ sc_status get_ctx(int device, DeviceCtx** out) {
   }
   if (device < 0 || device >= count)
     return fail(SC_ERR_INVALID_ARG, "device %d out of range (%d devices)", device, count);
-  std::lock_guard<std::mutex> lk(g_ctx_mu);
-  if ((int)g_ctx.size() < count) g_ctx.resize(count, nullptr);
+  return SC_OK;
+}
+
+sc_status create_ctx(int device, DeviceCtx** out) {
+  SC_TRY(count_devices(device));
   SC_CUDA(cudaSetDevice(device));
-  if (!g_ctx[device]) {
-    DeviceCtx* c = new DeviceCtx();
-    c->device = device;
+  DeviceCtx* c = new DeviceCtx();
+  c->device = device;
+  auto init = [&]() -> sc_status {
     SC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     SC_CUDA(cudaEventCreateWithFlags(&c->last_use, cudaEventDisableTiming));
     SC_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -124,8 +112,43 @@ sc_status get_ctx(int device, DeviceCtx** out) {
       SC_CUDA(cudaEventCreateWithFlags(&c->ev_out[i], cudaEventDisableTiming));
       SC_CUDA(cudaEventCreateWithFlags(&c->ev_d2h[i], cudaEventDisableTiming));
     }
-    g_ctx[device] = c;
+    return SC_OK;
+  };
+  const sc_status st = init();
+  if (st != SC_OK) {
+    destroy_ctx(c);
+    return st;
   }
+  *out = c;
+  return SC_OK;
+}
+
+void destroy_ctx(DeviceCtx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (cudaStream_t s : {c->h2d_stream, c->d2h_stream})
+    if (s) cudaStreamSynchronize(s);
+  for (Buf* b : c->all_bufs()) b->release();
+  for (cudaStream_t s : {c->stream, c->h2d_stream, c->d2h_stream})
+    if (s) cudaStreamDestroy(s);
+  if (c->last_use) cudaEventDestroy(c->last_use);
+  for (int i = 0; i < 2; ++i)
+    for (cudaEvent_t e : {c->ev_h2d[i], c->ev_xfree[i], c->ev_out[i], c->ev_d2h[i]})
+      if (e) cudaEventDestroy(e);
+  if (c->pinned_small) cudaFreeHost(c->pinned_small);
+  if (c->pinned_col) cudaFreeHost(c->pinned_col);
+  delete c;
+}
+
+sc_status get_ctx(int device, DeviceCtx** out) {
+  SC_TRY(count_devices(device));
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  int count = 0;
+  cudaGetDeviceCount(&count);
+  if ((int)g_ctx.size() < count) g_ctx.resize(count, nullptr);
+  SC_CUDA(cudaSetDevice(device));
+  if (!g_ctx[device]) SC_TRY(create_ctx(device, &g_ctx[device]));
   *out = g_ctx[device];
   return SC_OK;
 }
@@ -133,20 +156,7 @@ sc_status get_ctx(int device, DeviceCtx** out) {
 void release_all() {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   for (DeviceCtx*& c : g_ctx) {
-    if (!c) continue;
-    cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
-    for (Buf* b : c->all_bufs()) b->release();
-    if (c->stream) cudaStreamDestroy(c->stream);
-    if (c->last_use) cudaEventDestroy(c->last_use);
-    if (c->pinned_small) cudaFreeHost(c->pinned_small);
-    if (c->pinned_col) cudaFreeHost(c->pinned_col);
-    for (cudaStream_t s : {c->h2d_stream, c->d2h_stream})
-      if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
-    for (int i = 0; i < 2; ++i)
-      for (cudaEvent_t e : {c->ev_h2d[i], c->ev_xfree[i], c->ev_out[i], c->ev_d2h[i]})
-        if (e) cudaEventDestroy(e);
-    delete c;
+    destroy_ctx(c);
     c = nullptr;
   }
 }
@@ -279,6 +289,7 @@ struct Problem {
   int mode = 2; T lambda1 = 0; int pos = 0; int length_path = 0;
   int Lsig = 0; T eps = 0, lambda = 0;
   const int* dLv = nullptr; const T* dEps = nullptr; const T* dLam = nullptr;
+  const T* dLam1 = nullptr;       // per-signal lambda1 of the Lasso, or nullptr
   // device CSC output (device entry points); unused with a host sink
   int64_t* d_colptr = nullptr; int32_t* d_rows = nullptr; T* d_vals = nullptr;
   int64_t cap = 0;
@@ -493,6 +504,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       LarsArgs<T> a{};
       a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
       a.Lcap = shp.Lcap; a.mode = p.mode; a.constraint = p.lambda1; a.pos = p.pos;
+      a.vConstraint = p.dLam1 ? p.dLam1 + start : nullptr;
       a.length_path = p.length_path; a.n_jobs = (int)cn; a.n_jobs_dev = nullptr;
       a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
       a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
@@ -629,7 +641,7 @@ static sc_status emit_sink(int64_t m, int64_t n, HostSink<T>& s, typename CscOf<
 static inline int pad128(int K) { return ((K + 127) / 128) * 128; }
 // Padded atom count: a multiple of 128 up to 1024 atoms (one warp per signal),
 // of 512 beyond (one CTA of Kp / 512 warps per signal).
-static inline int pad_atoms(int K) {
+int pad_atoms(int K) {
   const int p = pad128(K);
   return p <= kWarpMaxKp ? p : ((K + 511) / 512) * 512;
 }
@@ -690,7 +702,7 @@ static sc_status check_tc(DeviceCtx& c, cudaStream_t st, const Problem<T>& p) {
   return SC_OK;
 }
 
-static sc_status check_kp(int K) {
+sc_status check_atoms(int K) {
   if (pad_atoms(K) > kCtaMaxKp)
     return fail(SC_ERR_UNSUPPORTED, "dictionaries with more than %d atoms are not supported (K=%d)",
                 kCtaMaxKp, K);
@@ -729,7 +741,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (L <= 0) return emit_empty<T>(0, 0, out);  // spalpha.clear(); return
   L = std::min(m, std::min(L, K));
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
-  SC_TRY(check_kp(K));
+  SC_TRY(check_atoms(K));
 
   SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
@@ -829,7 +841,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (path) memset(path, 0, sizeof(T) * (size_t)K * std::max(0, max_length_path));
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);
-  SC_TRY(check_kp(K));
+  SC_TRY(check_atoms(K));
 
   SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
@@ -915,7 +927,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
     return fail(SC_ERR_INVALID_ARG, "lasso : null device pointer");
   if (mode < 0 || mode > 2) return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
-  SC_TRY(check_kp(K));
+  SC_TRY(check_atoms(K));
   SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
@@ -956,7 +968,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   if (m <= 0 || n < 0 || K <= 0) return fail(SC_ERR_INVALID_ARG, "omp : bad dimensions");
   if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
     return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
-  SC_TRY(check_kp(K));
+  SC_TRY(check_atoms(K));
   SC_TRY(check_opts<T>(opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
@@ -988,6 +1000,56 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
+}
+
+// ---------------------------------------------------------------------------
+// batches of device-resident signals (the serving slots)
+sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b) {
+  cudaStream_t st = c.stream;
+  SC_TRY(c.misc.reserve(MISC_BYTES));
+  int* d_capflag = misc_at<int>(c.misc, MISC_CAPFLAG);
+  SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
+  Problem<float> p;
+  p.lars = b.lars; p.dX = b.dX; p.dD = b.dD; p.m = b.m; p.n = b.n; p.K = b.K; p.Kp = b.Kp;
+  p.L = b.L; p.mode = b.mode; p.lambda1 = b.lambda1; p.pos = b.pos;
+  p.length_path = b.length_path; p.dLam1 = b.dLam1;
+  p.Lsig = b.Lsig; p.eps = b.eps; p.lambda = b.lambda;
+  p.dLv = b.dLv; p.dEps = b.dEps; p.dLam = b.dLam;
+  p.d_colptr = b.d_colptr; p.d_rows = b.d_rows; p.d_vals = b.d_vals; p.cap = b.cap;
+  p.refine = b.refine;
+  if (b.tc) {
+    if (!b.dDsplit) return fail(SC_ERR_INVALID_ARG, "batch: BF16 products without the split dictionary");
+    p.tc = true;
+    p.mp = tc_pad_m(b.m);
+    p.dDsplit = b.dDsplit;
+    p.d_tc_err = misc_at<int>(c.misc, MISC_TC_ERR);
+    SC_CUDA(cudaMemsetAsync(p.d_tc_err, 0, 4, st));
+  }
+  if (b.n == 0) {
+    SC_CUDA(cudaMemsetAsync(b.d_colptr, 0, 8, st));
+    return SC_OK;
+  }
+  Prof pr;
+  pr.st = st;
+  return run_pipeline<float>(c, st, p, b.G, nullptr, d_capflag, pr);
+}
+
+sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz) {
+  int64_t* h = reinterpret_cast<int64_t*>(c.pinned_small);
+  SC_CUDA(cudaMemcpyAsync(h, b.d_colptr + b.n, 8, cudaMemcpyDeviceToHost, c.stream));
+  SC_CUDA(cudaMemcpyAsync(h + 1, misc_at<int>(c.misc, MISC_CAPFLAG), 4, cudaMemcpyDeviceToHost,
+                          c.stream));
+  int* herr = reinterpret_cast<int*>(h + 2);
+  *herr = 0;
+  if (b.tc)
+    SC_CUDA(cudaMemcpyAsync(herr, misc_at<int>(c.misc, MISC_TC_ERR), 4, cudaMemcpyDeviceToHost,
+                            c.stream));
+  SC_CUDA(cudaStreamSynchronize(c.stream));
+  *nnz = h[0];
+  if (*reinterpret_cast<int*>(h + 1))
+    return fail(SC_ERR_CAPACITY, "batch output capacity too small: nnz = %lld", (long long)h[0]);
+  if (*herr) return fail(SC_ERR_TIMEOUT, "tensor-core correlation pipeline: a bounded wait gave up");
+  return SC_OK;
 }
 
 }  // namespace sc

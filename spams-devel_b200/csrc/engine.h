@@ -14,6 +14,23 @@ namespace sc {
 sc_status fail(sc_status st, const char* fmt, ...);
 const char* last_error();
 
+#define SC_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t _e = (call);                                                       \
+    if (_e != cudaSuccess)                                                         \
+      return fail(_e == cudaErrorMemoryAllocation ? SC_ERR_OUT_OF_MEMORY          \
+                                                  : SC_ERR_CUDA,                   \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
+                  __LINE__);                                                       \
+  } while (0)
+
+#define SC_TRY(expr)                    \
+  do {                                  \
+    sc_status _s = (expr);              \
+    if (_s != SC_OK) return _s;         \
+  } while (0)
+
+
 // A grow-only device allocation cached between calls.
 struct Buf {
   void* ptr = nullptr;
@@ -51,5 +68,43 @@ struct DeviceCtx {
 
 sc_status get_ctx(int device, DeviceCtx** out);
 void release_all();
+// A private context (own streams and workspaces), not shared with the C ABI
+// calls; the serving slots each own one.
+sc_status create_ctx(int device, DeviceCtx** out);
+void destroy_ctx(DeviceCtx* c);
+
+// One coding launch over signals already on the device (float32), with
+// per-signal parameters; the CSC goes to caller-owned device arrays.  Enqueued
+// on c.stream; finish_batch waits for it and checks its status flags.
+struct BatchDesc {
+  bool lars = true;
+  const float* dX = nullptr;   // m x n, column-major
+  int m = 0;
+  int64_t n = 0;
+  const float* dD = nullptr;   // m x K
+  const float* G = nullptr;    // Kp x Kp Gram (with the ridge for the Lasso)
+  const void* dDsplit = nullptr;  // BF16 hi / lo halves of D (tc), or NULL
+  int K = 0, Kp = 0;
+  int L = 0;                   // slab stride: the largest L of the batch
+  // Lasso
+  int mode = 2, pos = 0, length_path = -1;
+  float lambda1 = 0;
+  const float* dLam1 = nullptr;   // per-signal lambda1
+  // OMP
+  int Lsig = 0;
+  float eps = 0, lambda = 0;
+  const int* dLv = nullptr;
+  const float* dEps = nullptr;
+  const float* dLam = nullptr;
+  bool tc = false, refine = false;
+  int64_t* d_colptr = nullptr;
+  int32_t* d_rows = nullptr;
+  float* d_vals = nullptr;
+  int64_t cap = 0;
+};
+sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b);
+sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz);
+int pad_atoms(int K);
+sc_status check_atoms(int K);
 
 }  // namespace sc

@@ -35,6 +35,7 @@ struct LarsArgs {
   int Lcap;            // active-set capacity of the per-warp state
   int mode;            // 0 L1COEFFS, 1 L2ERROR, 2 PENALTY
   T constraint;        // lambda1
+  const T* vConstraint;  // per-signal lambda1 (device) or NULL
   int pos;
   int length_path;
   int n_jobs;          // signals in this launch

@@ -81,7 +81,6 @@ lars_kernel(const LarsArgs<T> a) {
   const int L = a.L < K ? a.L : K;  // L = MIN(LL, K)
   const int length_path = a.length_path <= 1 ? 4 * L : a.length_path;
   const int mode = a.mode;
-  const T constraint = a.constraint;
   const bool pos = a.pos != 0;
 
   const int n_jobs = a.n_jobs_dev ? *a.n_jobs_dev : a.n_jobs;
@@ -98,6 +97,7 @@ lars_kernel(const LarsArgs<T> a) {
     job = __shfl_sync(kFull, job, 0);
     if (job >= n_jobs) break;
     const int64_t sig = a.sig_list ? a.sig_list[job] : (int64_t)job;
+    const T constraint = a.vConstraint ? a.vConstraint[sig] : a.constraint;
     T* path = (a.path && sig == 0) ? a.path : nullptr;
 
     // ---- load D^T x and find the first atom

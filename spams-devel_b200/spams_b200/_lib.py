@@ -32,7 +32,13 @@ EXPORTS = (
     "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
     "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
     "sc_last_profile", "sc_corr_f32_dev", "sc_corr_bf16x3_noalloc_f32",
+    "sc_server_create", "sc_server_destroy", "sc_server_add_dictionary_f32",
+    "sc_server_remove_dictionary", "sc_server_submit", "sc_server_wait", "sc_server_replay",
+    "sc_server_stats_get",
 )
+
+SC_REQ_OMP, SC_REQ_LASSO = 0, 1
+SC_REQ_DISCARD = 1
 
 
 class CscF32(C.Structure):
@@ -58,6 +64,23 @@ class Profile(C.Structure):
                 ("ms_total", C.c_double),
                 ("launches", C.c_int64), ("signals", C.c_int64), ("steps", C.c_int64),
                 ("overflowed", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Request(C.Structure):
+    _fields_ = [("dict_id", C.c_int64), ("algo", C.c_int), ("X", C.c_void_p), ("n", C.c_int64),
+                ("L", C.c_int), ("eps", C.c_float), ("lambda1", C.c_float), ("mode", C.c_int),
+                ("pos", C.c_int), ("precision", C.c_int), ("refine", C.c_int), ("flags", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("signals", C.c_int64), ("batches", C.c_int64),
+                ("rejected", C.c_int64), ("pending", C.c_int64),
+                ("lat_p50_ms", C.c_double), ("lat_p99_ms", C.c_double),
+                ("lat_mean_ms", C.c_double), ("lat_max_ms", C.c_double), ("busy_s", C.c_double),
+                ("peak_device_bytes", C.c_int64), ("mean_batch_requests", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -115,6 +138,14 @@ def lib() -> C.CDLL:
                                    i64p, p, opt]),
         "sc_corr_f32_dev": (i32, [p, i32, i32, p, i64, p, i32, i32, p]),
         "sc_corr_bf16x3_noalloc_f32": (i32, [p, i32, i32, p, i64, p, i32, p]),
+        "sc_server_create": (i32, [i32, i64, i32, i64, C.POINTER(p)]),
+        "sc_server_destroy": (i32, [p]),
+        "sc_server_add_dictionary_f32": (i32, [p, i64, f32p, i32, i32]),
+        "sc_server_remove_dictionary": (i32, [p, i64]),
+        "sc_server_submit": (i32, [p, C.POINTER(Request), i64p]),
+        "sc_server_wait": (i32, [p, i64, d, C.POINTER(CscF32), C.POINTER(C.c_double)]),
+        "sc_server_replay": (i32, [p, C.POINTER(Request), f64p, i64]),
+        "sc_server_stats_get": (i32, [p, i32, C.POINTER(ServerStats)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)

@@ -93,3 +93,45 @@ def smooth_patches(n: int, rng: np.random.Generator, side: int = 12) -> np.ndarr
     P = Z.reshape(n, side * side).T
     P = P - P.mean(axis=0, keepdims=True)
     return np.asfortranarray(unit_columns(P))
+
+
+# the eight resident dictionaries of the serving workload: every m of
+# {64, 144, 256, 512} with two atom counts of {256, 1024, 2048, 4096}
+SERVING_DICTS = ((64, 256), (64, 1024), (144, 256), (144, 1024), (256, 1024), (256, 2048),
+                 (512, 2048), (512, 4096))
+
+
+def config_serving(rate: float = 2000.0, duration_s: float = 10.0, seed: int = 0,
+                   pool: int = 50000, nmax: int = 50000, noise: float = 0.01):
+    """Serving stream: Poisson arrivals at `rate` requests/s for duration_s;
+    each request picks one of the eight dictionaries uniformly (unit-norm
+    N(0,1)), n ~ log-uniform on [1, nmax] signals, and OMP with L ~ U{4..32}
+    or Lasso (mode 2) with lambda1 ~ U[0.05, 0.3] at equal odds.  Signals are
+    sparse combinations D a + 0.01 N(0,1) with s ~ U{1..16} non-zeros, drawn
+    once into a pool of `pool` float32 columns per dictionary; a request codes
+    a random contiguous window of its dictionary's pool.
+
+    Returns (dicts, pools, reqs) with dicts a list of m x K float32 arrays,
+    pools the matching m x pool float32 arrays, and reqs a dict of per-request
+    arrays: arrival_s, dict, n, offset, algo (0 OMP / 1 Lasso), L, lambda1."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dicts, pools = [], []
+    for m, K in SERVING_DICTS:
+        D = gaussian_dictionary(m, K, rng)
+        s = rng.integers(1, 17, size=pool)
+        X, _, _ = sparse_signals(D, pool, s, noise, rng)
+        dicts.append(np.asfortranarray(D, dtype=np.float32))
+        pools.append(np.asfortranarray(X, dtype=np.float32))
+    count = max(1, int(rng.poisson(rate * duration_s)))
+    arrival = np.sort(rng.random(count) * duration_s)
+    dsel = rng.integers(0, len(SERVING_DICTS), size=count)
+    nreq = np.minimum(nmax, np.floor(np.exp(rng.random(count) * np.log(nmax + 1))).astype(np.int64))
+    nreq = np.maximum(nreq, 1)
+    nreq = np.minimum(nreq, pool)
+    offset = (rng.random(count) * (pool - nreq + 1)).astype(np.int64)
+    algo = rng.integers(0, 2, size=count)
+    L = rng.integers(4, 33, size=count)
+    lam = 0.05 + 0.25 * rng.random(count)
+    reqs = {"arrival_s": arrival, "dict": dsel, "n": nreq, "offset": offset, "algo": algo,
+            "L": L, "lambda1": lam}
+    return dicts, pools, reqs
