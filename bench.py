@@ -8,14 +8,24 @@ the whole batch: Gram, ||x||^2, D^T X, the LARS homotopy of every signal and
 the CSC assembly.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision bf16x3|fp32] [--workload lasso|uneven_omp|serve]
 
 `value` is measured through the device entry point with inputs resident in
 HBM (CUDA events on the call's stream, an L2-flushing write between steps);
 `e2e` through the host entry point with pinned host buffers, copies inside
-the timed region.  With N > 1 (torchrun) every rank codes its own batch with
-the same dictionary (weak scaling, no collective on the data path); rank 0
-prints the aggregate.  `--impl reference` times the SPAMS reference's own CPU
-code (oracle/_ref) on the host cores instead.
+the timed region.  The correlations D^T X run as BF16 hi/lo tensor-core
+products (FP32-grade, see the parity tests) unless --precision fp32; the
+plain FP32 path is timed beside it (`fp32_value`).  With N > 1 (torchrun)
+every rank codes its own batch with the same dictionary (weak scaling, no
+collective on the data path); rank 0 prints the aggregate.  `--impl
+reference` times the SPAMS reference's own CPU code (oracle/_ref) on the host
+cores instead.
+
+Two more workloads, each printing its own JSON line (one GPU):
+  --workload uneven_omp  batched uneven OMP: D 512 x 2048, X 512 x 1e6,
+                         s_i ~ U{1..64}, L_i = s_i + 4, eps_i = 0.5 ||noise_i||^2
+  --workload serve       serving stream: Poisson arrivals at --rate req/s over
+                         eight resident dictionaries, p50 / p99 latency
 """
 from __future__ import annotations
 
@@ -175,7 +185,8 @@ def run_reference(args) -> None:
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": config_dict(args.n, args.gpus, "fp32"),
+        "config": dict(config_dict(args.n, args.gpus, args.precision),
+                       precision="reference float build on the host cores"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{sample} of the {args.n} signals per step, "
                                    f"reference lasso2 float build, OpenMP {threads} threads, "
@@ -250,6 +261,30 @@ def run_ours(args) -> None:
     total_ms = float(t.item())
     nnz = int(outs[0][n].item())
 
+    # ---- the plain FP32 path on the same inputs, same timing rules
+    fp32_ms = None
+    if prec != spams_b200.SC_PREC_FP32:
+        def step32():
+            return spams_b200.lasso_device(Xt, Dt, LAMBDA, stream=stream,
+                                           precision=spams_b200.SC_PREC_FP32, out=outs,
+                                           sync=False)
+        for _ in range(2):
+            step32()
+        barrier()
+        evs32 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                 for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evs32[i][0].record(stream)
+            step32()
+            evs32[i][1].record(stream)
+        barrier()
+        t = torch.tensor([sum(a.elapsed_time(b) for a, b in evs32)], dtype=torch.float64,
+                         device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fp32_ms = float(t.item())
+
     # ---- timed region B: per-stage device times of the same call
     stage = {"ms_gram": 0.0, "ms_norms": 0.0, "ms_corr": 0.0, "ms_code": 0.0, "ms_refine": 0.0,
              "ms_csc": 0.0, "steps": 0, "overflowed": 0}
@@ -323,6 +358,7 @@ def run_ours(args) -> None:
                      "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
         "stages_ms": {k: stage[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
                                             "ms_refine", "ms_csc")},
+        "fp32_value": (world * n * args.steps / (fp32_ms / 1e3)) if fp32_ms else value,
         "homotopy_steps_per_signal": stage["steps"] / n,
         "nnz_per_signal": nnz / n,
         "overflowed_signals": stage["overflowed"],
@@ -334,19 +370,262 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# batched uneven OMP (D 512 x 2048, X 512 x 1e6)
+
+UO_M, UO_K = 512, 2048
+UO_METRIC = ("coded signals/s (batched uneven OMP, D 512x2048, s~U{1..64}, L=s+4, "
+             "eps=0.5||noise||^2)")
+
+
+def run_uneven_omp(args) -> None:
+    import torch
+    import spams_b200
+    from spams_b200 import workloads as W
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
+    n = args.n or 1000000
+    X, D, Lv, eps = W.config_uneven_omp_device(n=n, seed=0, m=UO_M, K=UO_K, device=dev)
+    Lmax = int(Lv.max().item())
+    cap = n * Lmax
+    outs = (torch.empty(n + 1, dtype=torch.int64, device=dev),
+            torch.empty(cap, dtype=torch.int32, device=dev),
+            torch.empty(cap, dtype=torch.float32, device=dev))
+    stream = torch.cuda.current_stream(dev)
+
+    def step(profile=False, p=prec):
+        return spams_b200.omp_device(X, D, L=Lmax, L_vec=Lv, eps_vec=eps, stream=stream,
+                                     precision=p, out=outs, sync=False, profile=profile)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # inputs (2 GB of X, 8 GB of correlations per pass) exceed L2
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    launches = 0
+    with Clocks(0) as clk:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            evs[i][0].record(stream)
+            step()
+            evs[i][1].record(stream)
+            launches += spams_b200.last_profile()["launches"]
+        torch.cuda.synchronize()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    nnz = int(outs[0][n].item())
+    fp32_ms = None
+    if prec != spams_b200.SC_PREC_FP32:
+        step(p=spams_b200.SC_PREC_FP32)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(p=spams_b200.SC_PREC_FP32)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp32_ms = e0.elapsed_time(e1)
+    stage = {"ms_corr": 0.0, "ms_code": 0.0, "ms_csc": 0.0, "ms_norms": 0.0, "ms_gram": 0.0,
+             "ms_refine": 0.0, "steps": 0, "overflowed": 0}
+    step(profile=True)
+    p = spams_b200.last_profile()
+    for k in stage:
+        stage[k] = p[k]
+    # end to end: host arrays (pinned) in, CSC on the host out
+    Xh = torch.empty((n, UO_M), dtype=torch.float32, pin_memory=True)
+    Xh.copy_(X.t())
+    Xnp = Xh.numpy().T
+    Dnp = np.asfortranarray(D.cpu().numpy())
+    Lnp, Enp = Lv.cpu().numpy(), eps.cpu().numpy()
+    spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        a = spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            O.build_ref()
+            cal = 500
+            t0 = time.perf_counter()
+            O.ref_omp(Xnp[:, :cal], Dnp, L=Lnp[:cal], eps=Enp[:cal], numThreads=-1)
+            dt = max(time.perf_counter() - t0, 1e-6)
+            sample = int(min(n, max(cal, cal * args.cpu_seconds / dt)))
+            t0 = time.perf_counter()
+            O.ref_omp(np.asfortranarray(Xnp[:, :sample]), Dnp, L=Lnp[:sample], eps=Enp[:sample],
+                      numThreads=-1)
+            rate = sample / (time.perf_counter() - t0)
+            thr = omp_threads(-1)
+            cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "reference",
+                   "sample": f"first {sample} signals, reference omp (T=float), OpenMP {thr} "
+                             "threads, OPENBLAS_NUM_THREADS=1"}
+        except Exception as e:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    peaks = measured_peaks()
+    code_ms = stage["ms_code"]
+    # per signal: the K-float correlation column, one K-float Gram column per
+    # selected atom, the (index, value) pair of each coefficient
+    alg_bytes = 4 * UO_K * n + 4 * UO_K * stage["steps"] + 8 * nnz
+    achieved = alg_bytes / (code_ms / 1e3) / 1e9 if code_ms > 0 else None
+    value = n * args.steps / (total_ms / 1e3)
+    line = {
+        "metric": UO_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded, drawn on the device)",
+        "config": {"workload": f"uneven_omp_D{UO_M}x{UO_K}_n{n}_s1-64_noise0.02",
+                   "m": UO_M, "K": UO_K, "n": n, "precision": args.precision,
+                   "between_steps": "inputs larger than L2 (2 GB of X)",
+                   "parallelism": "one GPU"},
+        "e2e": {"value": n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Xnp.nbytes + Dnp.nbytes
+                + Lnp.nbytes + Enp.nbytes, "d2h_bytes_per_step": (n + 1) * 8 + a.nnz * 8},
+        "gpu_launches": launches,
+        "roofline": {"kernel": "omp_cta_kernel", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+                     "traffic": None, "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
+        "stages_ms": {k: stage[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
+                                            "ms_refine", "ms_csc")},
+        "fp32_value": (n * args.steps / (fp32_ms / 1e3)) if fp32_ms else value,
+        "omp_steps_per_signal": stage["steps"] / n, "nnz_per_signal": nnz / n,
+        "overflowed_signals": stage["overflowed"],
+        "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# serving stream
+
+SERVE_METRIC = ("p99 request latency (serving stream: Poisson arrivals over 8 resident "
+                "dictionaries, n log-uniform 1..5e4, OMP L~U{4..32} or Lasso lambda1~U[0.05,0.3])")
+
+
+def _serve_requests(pools, rate, duration, seed, prec):
+    import spams_b200
+    rng = np.random.Generator(np.random.PCG64(seed))
+    count = max(1, int(rng.poisson(rate * duration)))
+    arrival = np.sort(rng.random(count) * duration)
+    dsel = rng.integers(0, len(pools), size=count)
+    pool = pools[0].shape[1]
+    n = np.maximum(1, np.minimum(pool, np.floor(np.exp(rng.random(count) * np.log(50001)))
+                                 .astype(np.int64)))
+    off = (rng.random(count) * (pool - n + 1)).astype(np.int64)
+    algo = rng.integers(0, 2, size=count)
+    L = rng.integers(4, 33, size=count)
+    lam = 0.05 + 0.25 * rng.random(count)
+    recs = []
+    for k in range(count):
+        Xk = pools[dsel[k]][:, off[k]:off[k] + n[k]]
+        if algo[k] == 0:
+            recs.append(spams_b200.request(int(dsel[k]), Xk, "omp", L=int(L[k]), precision=prec,
+                                           discard=True))
+        else:
+            recs.append(spams_b200.request(int(dsel[k]), Xk, "lasso", lambda1=float(lam[k]),
+                                           precision=prec, discard=True))
+    return recs, arrival, int(n.sum())
+
+
+def run_serve(args) -> None:
+    import torch
+    import spams_b200
+    from spams_b200 import workloads as W
+    torch.cuda.set_device(0)
+    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
+    dicts, pools, _ = W.config_serving(rate=1.0, duration_s=1.0, seed=0)
+    pinned = []
+    for P in pools:  # request signals live in pinned host memory
+        h = torch.empty((P.shape[1], P.shape[0]), dtype=torch.float32, pin_memory=True)
+        h.numpy()[:] = P.T
+        pinned.append(h.numpy().T)
+    out = {}
+    with spams_b200.Server(hbm_budget=150e9, slots=args.slots) as srv:
+        for i, D in enumerate(dicts):
+            srv.add_dictionary(i, D)
+        # warm-up: one second of the stream (kernels loaded, workspaces grown)
+        recs, arr, _ = _serve_requests(pinned, args.rate, 1.0, 99, prec)
+        srv.replay(recs, arr)
+        sweep = []
+        rates = [args.rate] + ([r for r in (250.0, 500.0, 1000.0) if r < args.rate]
+                               if not args.no_sweep else [])
+        clk_summary = None
+        for rate in rates:
+            recs, arr, offered = _serve_requests(pinned, rate, args.duration, int(rate), prec)
+            srv.stats(reset=True)
+            with Clocks(0) as clk:
+                t0 = time.perf_counter()
+                srv.replay(recs, arr)
+                wall = time.perf_counter() - t0
+            st = srv.stats(reset=True)
+            if clk_summary is None:
+                clk_summary = clk.summary()
+            sweep.append({"rate_req_s": rate, "requests": len(recs),
+                          "offered_signals_s": offered / args.duration,
+                          "served_signals_s": st["signals"] / wall, "wall_s": wall,
+                          "p50_ms": st["lat_p50_ms"], "p99_ms": st["lat_p99_ms"],
+                          "mean_ms": st["lat_mean_ms"], "max_ms": st["lat_max_ms"],
+                          "requests_per_launch": st["mean_batch_requests"],
+                          "rejected": st["rejected"], "gpu_busy_s": st["busy_s"],
+                          "peak_device_bytes": st["peak_device_bytes"]})
+        out = sweep[0]
+    line = {
+        "metric": SERVE_METRIC, "value": out["p99_ms"], "unit": "ms", "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": out["wall_s"] * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; signals drawn once into per-dictionary pools)",
+        "config": {"workload": f"serving_poisson{args.rate:g}rps_{args.duration:g}s",
+                   "dictionaries": [list(t) for t in W.SERVING_DICTS], "slots": args.slots,
+                   "hbm_budget_bytes": 150e9, "precision": args.precision,
+                   "between_steps": "inputs larger than L2 (pools of 0.39 GB)",
+                   "parallelism": "one GPU"},
+        "p50_ms": out["p50_ms"], "served_signals_s": out["served_signals_s"],
+        "offered_signals_s": out["offered_signals_s"],
+        "e2e": {"value": out["p99_ms"], "unit": "ms", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "sweep": sweep, "clocks": clk_summary,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=100000, help="signals per GPU")
-    ap.add_argument("--precision", choices=["fp32", "bf16x3"], default="fp32")
+    ap.add_argument("--workload", choices=["lasso", "uneven_omp", "serve"], default="lasso")
+    ap.add_argument("--n", type=int, default=None, help="signals per GPU")
+    ap.add_argument("--precision", choices=["fp32", "bf16x3"], default="bf16x3")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-step-s", type=float, default=5.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: requests/s")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=3, help="serve: concurrent launches")
+    ap.add_argument("--no-sweep", action="store_true", help="serve: skip the lower rates")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed steps
+    if args.workload == "uneven_omp":
+        if args.impl == "ours":
+            run_uneven_omp(args)
+        else:
+            print(json.dumps({"impl": "reference", "metric": UO_METRIC,
+                              "unavailable": "reference arm is timed on the lasso workload"}))
+        return 0
+    if args.workload == "serve":
+        if args.impl == "ours":
+            run_serve(args)
+        else:
+            print(json.dumps({"impl": "reference", "metric": SERVE_METRIC,
+                              "unavailable": "the reference has no serving loop"}))
+        return 0
+    args.n = args.n or 100000
     if args.impl == "reference":
         run_reference(args)
     else:

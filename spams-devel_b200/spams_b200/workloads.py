@@ -135,3 +135,36 @@ def config_serving(rate: float = 2000.0, duration_s: float = 10.0, seed: int = 0
     reqs = {"arrival_s": arrival, "dict": dsel, "n": nreq, "offset": offset, "algo": algo,
             "L": L, "lambda1": lam}
     return dicts, pools, reqs
+
+
+def config_uneven_omp_device(n: int = 1000000, seed: int = 0, m: int = 512, K: int = 2048,
+                             smax: int = 64, noise: float = 0.02, device=None,
+                             chunk: int = 1 << 16):
+    """config_uneven_omp drawn on a CUDA device with torch (for the full-size
+    run, whose host draw takes minutes): same shapes and distributions (unit
+    D, s_i ~ U{1..smax} distinct atoms with N(0,1) values, 0.02 N(0,1) noise,
+    L_i = s_i + 4, eps_i = 0.5 ||noise_i||^2), a different random stream.
+    Returns float32 CUDA tensors X (m x n, column-major view), D (m x K,
+    column-major view), L (int32) and eps."""
+    import torch
+    dev = torch.device(device if device is not None else "cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    D = torch.randn((K, m), generator=g, device=dev, dtype=torch.float32)
+    D = D / D.norm(dim=1, keepdim=True)
+    s = torch.randint(1, smax + 1, (n,), generator=g, device=dev)
+    Xr = torch.empty((n, m), device=dev, dtype=torch.float32)
+    eps = torch.empty(n, device=dev, dtype=torch.float32)
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        w = torch.ones((c1 - c0, K), device=dev)
+        idx = torch.multinomial(w, smax, replacement=False, generator=g)
+        vals = torch.randn((c1 - c0, smax), generator=g, device=dev)
+        vals = vals * (torch.arange(smax, device=dev)[None, :] < s[c0:c1, None])
+        A = torch.zeros((c1 - c0, K), device=dev)
+        A.scatter_(1, idx, vals)
+        E = noise * torch.randn((c1 - c0, m), generator=g, device=dev)
+        Xr[c0:c1] = A @ D + E
+        eps[c0:c1] = 0.5 * (E * E).sum(dim=1)
+    L = (s + 4).to(torch.int32)
+    return Xr.t(), D.t(), L, eps
