@@ -278,6 +278,32 @@ sc_status sc_server_replay(sc_server* s, const sc_request* reqs, const double* a
 /* Counters and latency percentiles since the last reset. */
 sc_status sc_server_stats_get(sc_server* s, int reset, sc_server_stats* out);
 
+/* ---- Dictionary-learning inner loop -------------------------------------
+ * The minibatch step of Trainer::train (dictLearn/dicts.h:526-603) on device
+ * arrays, float32: G = DᵀD + max(lambda2, 1e-10) I; the minibatch
+ * x_j = X[:, perm[(j + it * batch) % M]] (perm NULL: identity) with `it` read
+ * from the device counter *d_iter; its codes (mode as constraint_type:
+ * L1COEFFS / L2ERROR / PENALTY run coreLARS2 with constraint lambda1 and
+ * posAlpha; SPARSITY / L2ERROR2 / PENALTY2 run coreORMPB with L = lambda1,
+ * eps = lambda1 or lambda = lambda1; L = min(m, K) otherwise); then
+ * A <- beta A + gamma sum_j a_j a_jᵀ (K x K) and B <- beta B + gamma sum_j x_j a_jᵀ
+ * (m x K), column-major (either may be NULL: skipped); finally *d_iter += 1.
+ * Everything is enqueued on `stream` without host synchronisation, so a step
+ * can be captured in a CUDA graph once a first step has sized the workspaces.
+ * The ridge-only conjugate-gradient case of the reference (PENALTY with
+ * lambda1 = 0, lambda2 > 0) returns SC_ERR_UNSUPPORTED.  No counterpart in
+ * the reference's C API (Trainer runs this loop inside train()). */
+typedef struct sc_dl sc_dl;
+
+sc_status sc_dl_create(int device, int m, int K, int batch, int mode, float lambda1,
+                       float lambda2, int posAlpha, int precision, sc_dl** out);
+sc_status sc_dl_destroy(sc_dl* s);
+sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
+                         const int32_t* dperm, int64_t* d_iter, float* dA, float* dB, float beta,
+                         float gamma, void* stream);
+/* Device CSC (batch + 1 column pointers, rows, values) of the last step's codes. */
+sc_status sc_dl_codes(sc_dl* s, const int64_t** colptr, const int32_t** rows, const float** vals);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

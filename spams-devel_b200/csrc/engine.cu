@@ -1005,7 +1005,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
 // ---------------------------------------------------------------------------
 // batches of device-resident signals (the serving slots)
 sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b) {
-  cudaStream_t st = c.stream;
+  cudaStream_t st = b.stream;
   SC_TRY(c.misc.reserve(MISC_BYTES));
   int* d_capflag = misc_at<int>(c.misc, MISC_CAPFLAG);
   SC_CUDA(cudaMemsetAsync(d_capflag, 0, 4, st));
@@ -1035,16 +1035,17 @@ sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b) {
 }
 
 sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz) {
+  cudaStream_t st = b.stream;
   int64_t* h = reinterpret_cast<int64_t*>(c.pinned_small);
-  SC_CUDA(cudaMemcpyAsync(h, b.d_colptr + b.n, 8, cudaMemcpyDeviceToHost, c.stream));
+  SC_CUDA(cudaMemcpyAsync(h, b.d_colptr + b.n, 8, cudaMemcpyDeviceToHost, st));
   SC_CUDA(cudaMemcpyAsync(h + 1, misc_at<int>(c.misc, MISC_CAPFLAG), 4, cudaMemcpyDeviceToHost,
-                          c.stream));
+                          st));
   int* herr = reinterpret_cast<int*>(h + 2);
   *herr = 0;
   if (b.tc)
     SC_CUDA(cudaMemcpyAsync(herr, misc_at<int>(c.misc, MISC_TC_ERR), 4, cudaMemcpyDeviceToHost,
-                            c.stream));
-  SC_CUDA(cudaStreamSynchronize(c.stream));
+                            st));
+  SC_CUDA(cudaStreamSynchronize(st));
   *nnz = h[0];
   if (*reinterpret_cast<int*>(h + 1))
     return fail(SC_ERR_CAPACITY, "batch output capacity too small: nnz = %lld", (long long)h[0]);

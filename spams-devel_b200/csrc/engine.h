@@ -75,7 +75,7 @@ void destroy_ctx(DeviceCtx* c);
 
 // One coding launch over signals already on the device (float32), with
 // per-signal parameters; the CSC goes to caller-owned device arrays.  Enqueued
-// on c.stream; finish_batch waits for it and checks its status flags.
+// on b.stream; finish_batch waits for it and checks its status flags.
 struct BatchDesc {
   bool lars = true;
   const float* dX = nullptr;   // m x n, column-major
@@ -101,6 +101,7 @@ struct BatchDesc {
   int32_t* d_rows = nullptr;
   float* d_vals = nullptr;
   int64_t cap = 0;
+  cudaStream_t stream = nullptr;  // the stream to enqueue on (NULL: the legacy default stream)
 };
 sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b);
 sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz);

@@ -218,6 +218,7 @@ sc_status run_batch(sc_server* s, Slot& sl, SrvDict& d, std::vector<SrvReq*>& ba
   b.d_rows = reinterpret_cast<int32_t*>(sl.orows.ptr);
   b.d_vals = reinterpret_cast<float*>(sl.ovals.ptr);
   b.cap = N * (int64_t)Lmax;
+  b.stream = st;
   SC_TRY(code_batch_f32(c, b));
   int64_t nnz = 0;
   SC_TRY(finish_batch(c, b, &nnz));

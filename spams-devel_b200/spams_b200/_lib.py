@@ -34,7 +34,7 @@ EXPORTS = (
     "sc_last_profile", "sc_corr_f32_dev", "sc_corr_bf16x3_noalloc_f32",
     "sc_server_create", "sc_server_destroy", "sc_server_add_dictionary_f32",
     "sc_server_remove_dictionary", "sc_server_submit", "sc_server_wait", "sc_server_replay",
-    "sc_server_stats_get",
+    "sc_server_stats_get", "sc_dl_create", "sc_dl_destroy", "sc_dl_step_f32", "sc_dl_codes",
 )
 
 SC_REQ_OMP, SC_REQ_LASSO = 0, 1
@@ -146,6 +146,10 @@ def lib() -> C.CDLL:
         "sc_server_wait": (i32, [p, i64, d, C.POINTER(CscF32), C.POINTER(C.c_double)]),
         "sc_server_replay": (i32, [p, C.POINTER(Request), f64p, i64]),
         "sc_server_stats_get": (i32, [p, i32, C.POINTER(ServerStats)]),
+        "sc_dl_create": (i32, [i32, i32, i32, i32, i32, f, f, i32, i32, C.POINTER(p)]),
+        "sc_dl_destroy": (i32, [p]),
+        "sc_dl_step_f32": (i32, [p, p, p, i64, p, p, p, p, f, f, p]),
+        "sc_dl_codes": (i32, [p, C.POINTER(p), C.POINTER(p), C.POINTER(p)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)

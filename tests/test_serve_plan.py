@@ -49,3 +49,15 @@ def test_request_records_follow_the_facade_defaults():
         spams_b200.request(5, X, "lasso")
     with pytest.raises(ValueError, match="Fortran-ordered float32"):
         spams_b200.request(5, np.ones((4, 3)), "omp", L=2)
+
+
+def test_minibatch_step_argument_errors_need_no_device():
+    with pytest.raises(spams_b200.ScError) as e:
+        spams_b200.MinibatchStep(144, 256, 128, mode=7)
+    assert e.value.status == _lib.SC_ERR_UNSUPPORTED
+    # PENALTY with lambda1 = 0 and a ridge is the reference's conjugate-gradient case
+    with pytest.raises(spams_b200.ScError, match="conjugate-gradient"):
+        spams_b200.MinibatchStep(144, 256, 128, mode=2, lambda1=0.0, lambda2=0.1)
+    with pytest.raises(spams_b200.ScError) as e:
+        spams_b200.MinibatchStep(0, 256, 128)
+    assert e.value.status == _lib.SC_ERR_INVALID_ARG
