@@ -26,6 +26,9 @@ Two more workloads, each printing its own JSON line (one GPU):
                          s_i ~ U{1..64}, L_i = s_i + 4, eps_i = 0.5 ||noise_i||^2
   --workload serve       serving stream: Poisson arrivals at --rate req/s over
                          eight resident dictionaries, p50 / p99 latency
+  --workload dictlearn   online dictionary-learning minibatch step (12x12 patches,
+                         D 144 x 1024, batch 1024), one CUDA graph replay per
+                         minibatch, minibatches/s (--n minibatches, default 2000)
 """
 from __future__ import annotations
 
@@ -593,13 +596,168 @@ def run_serve(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# online dictionary-learning inner loop
+
+DL_M, DL_K, DL_BATCH, DL_LAMBDA = 144, 1024, 1024, 0.1
+DL_METRIC = ("minibatches/s (online dictionary-learning step: 1024 signals of 12x12 smooth "
+             "patches, D 144x1024 perturbed and renormalised per minibatch, Gram recomputed, "
+             "Lasso lambda1=0.1, A/B accumulations)")
+
+
+def run_dictlearn(args) -> None:
+    import torch
+    import spams_b200
+    from spams_b200 import workloads as W
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
+    nb = args.n or 2000  # minibatches
+    rng = np.random.Generator(np.random.PCG64(0))
+    pool = 200000
+    Xnp = W.smooth_patches(pool, rng, side=12).astype(np.float32)
+    D0 = Xnp[:, rng.choice(pool, DL_K, replace=False)]  # random signals, as train() starts
+    D0 = np.asfortranarray(D0 / np.linalg.norm(D0, axis=0, keepdims=True))
+    perm = torch.from_numpy(rng.permutation(pool).astype(np.int32)).to(dev)
+    Xd = torch.from_numpy(np.ascontiguousarray(Xnp.T)).to(dev).t()
+    U = torch.from_numpy(rng.standard_normal((DL_M, nb + 1)).astype(np.float32)).to(dev)
+    V = torch.from_numpy(rng.standard_normal((DL_K, nb + 1)).astype(np.float32)).to(dev)
+
+    def fresh():
+        Dd = torch.from_numpy(np.ascontiguousarray(D0.T)).to(dev).t()
+        A = torch.zeros((DL_K, DL_K), device=dev).t()
+        B = torch.zeros((DL_K, DL_M), device=dev).t()
+        it = torch.zeros(1, dtype=torch.int64, device=dev)
+        return Dd, A, B, it
+
+    step = spams_b200.MinibatchStep(DL_M, DL_K, DL_BATCH, lambda1=DL_LAMBDA, precision=prec)
+    Dd, A, B, it = fresh()
+
+    def body():
+        # the dictionary changes every minibatch: rank-1 perturbation (the
+        # minibatch's column of U, V, picked by the device counter), unit columns
+        u = U.index_select(1, it).squeeze(1)
+        v = V.index_select(1, it).squeeze(1)
+        Dd.add_(0.01 * torch.outer(u, v))
+        Dd.div_(Dd.norm(dim=0, keepdim=True))
+        step(Dd, Xd, it, perm=perm, A=A, B=B, beta=1.0, gamma=1.0 / DL_BATCH)
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(args.warmup):
+            body()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        body()
+    # ---- timed: nb minibatches, one graph replay each
+    Dd.copy_(torch.from_numpy(np.ascontiguousarray(D0.T)).to(dev).t())
+    A.zero_()
+    B.zero_()
+    it.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record()
+        for _ in range(nb):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1)
+    done = int(it.item())
+    # ---- the same loop without the graph (launch-bound comparison)
+    ne = min(nb, 200)
+    Dd, A, B, it = fresh()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(ne):
+        body()
+    e1.record()
+    torch.cuda.synchronize()
+    eager_ms = e0.elapsed_time(e1)
+    # ---- stage times of one eager step
+    step.profile(True)
+    body()
+    torch.cuda.synchronize()
+    prof = spams_b200.last_profile()
+    step.profile(False)
+    cp, rows, vals = step.codes()
+    nnz = int(cp[-1].item())
+    # ---- end to end: each minibatch copied in from pinned host memory, its
+    # code count read back
+    Xh = torch.empty((DL_BATCH * 50, DL_M), dtype=torch.float32, pin_memory=True)
+    Xh.numpy()[:] = Xnp[:, :DL_BATCH * 50].T
+    Xbuf = torch.empty((DL_BATCH, DL_M), device=dev).t()
+    it1 = torch.zeros(1, dtype=torch.int64, device=dev)
+    Dd, A, B, it = fresh()
+    ne2 = 50
+    t0 = time.perf_counter()
+    for i in range(ne2):
+        Xbuf.copy_(Xh[i * DL_BATCH:(i + 1) * DL_BATCH].t(), non_blocking=True)
+        it1.zero_()
+        step(Dd, Xbuf, it1, A=A, B=B, beta=1.0, gamma=1.0 / DL_BATCH)
+        c2 = step.codes()[0]
+        int(c2[-1].item())
+    e2e_s = (time.perf_counter() - t0) / ne2
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            O.build_ref()
+            Xb = np.asfortranarray(Xnp[:, :DL_BATCH])
+            reps, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < args.cpu_seconds and reps < 200:
+                O.ref_lasso(Xb, D0, lambda1=DL_LAMBDA, L=min(DL_M, DL_K), numThreads=-1)
+                reps += 1
+            rate = reps / (time.perf_counter() - t0)
+            thr = omp_threads(-1)
+            cpu = {"value": rate, "unit": "minibatches/s", "cores": thr, "kind": "reference",
+                   "sample": f"{reps} minibatches of {DL_BATCH} signals: reference lasso2 "
+                             f"(T=float, Gram recomputed per call), OpenMP {thr} threads; the "
+                             "A/B accumulations are not included"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "minibatches/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    peaks = measured_peaks()
+    code_ms = prof["ms_code"]
+    alg_bytes = 4 * DL_K * DL_BATCH + 4 * DL_K * prof["steps"] + 8 * nnz
+    achieved = alg_bytes / (code_ms / 1e3) / 1e9 if code_ms > 0 else None
+    value = done / (graph_ms / 1e3)
+    line = {
+        "metric": DL_METRIC, "value": value, "unit": "minibatches/s", "n_gpus": 1,
+        "steps": done, "warmup": args.warmup, "ms_per_step": graph_ms / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded smooth 12x12 patches, pool of 200000)",
+        "config": {"workload": f"dictlearn_m{DL_M}_K{DL_K}_batch{DL_BATCH}_lambda{DL_LAMBDA}",
+                   "minibatches": done, "precision": args.precision,
+                   "between_steps": "none (a minibatch's inputs are 0.6 MB; the loop is the unit)",
+                   "launch": "one CUDA graph replay per minibatch", "parallelism": "one GPU"},
+        "eager_value": ne / (eager_ms / 1e3),
+        "e2e": {"value": 1.0 / e2e_s, "unit": "minibatches/s",
+                "h2d_bytes_per_step": DL_BATCH * DL_M * 4, "d2h_bytes_per_step": 8},
+        "gpu_launches": None,
+        "roofline": {"kernel": "lars_kernel", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
+                     "traffic": None, "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
+        "stages_ms": {k: prof[k] for k in ("ms_norms", "ms_corr", "ms_code", "ms_csc")},
+        "homotopy_steps_per_signal": prof["steps"] / DL_BATCH, "nnz_per_signal": nnz / DL_BATCH,
+        "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lasso", "uneven_omp", "serve"], default="lasso")
+    ap.add_argument("--workload", choices=["lasso", "uneven_omp", "serve", "dictlearn"],
+                    default="lasso")
     ap.add_argument("--n", type=int, default=None, help="signals per GPU")
     ap.add_argument("--precision", choices=["fp32", "bf16x3"], default="bf16x3")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -624,6 +782,13 @@ def main() -> int:
         else:
             print(json.dumps({"impl": "reference", "metric": SERVE_METRIC,
                               "unavailable": "the reference has no serving loop"}))
+        return 0
+    if args.workload == "dictlearn":
+        if args.impl == "ours":
+            run_dictlearn(args)
+        else:
+            print(json.dumps({"impl": "reference", "metric": DL_METRIC,
+                              "unavailable": "reference arm is timed on the lasso workload"}))
         return 0
     args.n = args.n or 100000
     if args.impl == "reference":

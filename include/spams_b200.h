@@ -301,6 +301,10 @@ sc_status sc_dl_destroy(sc_dl* s);
 sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
                          const int32_t* dperm, int64_t* d_iter, float* dA, float* dB, float beta,
                          float gamma, void* stream);
+/* on != 0: later steps record the coding stages' device times, read with
+ * sc_last_profile on the calling thread (this synchronises the stream: not
+ * inside a graph capture). */
+sc_status sc_dl_profile(sc_dl* s, int on);
 /* Device CSC (batch + 1 column pointers, rows, values) of the last step's codes. */
 sc_status sc_dl_codes(sc_dl* s, const int64_t** colptr, const int32_t** rows, const float** vals);
 

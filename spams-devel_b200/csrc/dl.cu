@@ -136,6 +136,7 @@ struct sc_dl {
   float lambda1 = 0, lambda2 = 0;
   int pos = 0, precision = 0;
   int L = 0;
+  bool profile = false;
   DeviceCtx* ctx = nullptr;
   Buf G, Xb, split, colptr, rows, vals, cntK, ptrK, fillK, sigK, valK, sigT, valT, scan;
 };
@@ -262,6 +263,8 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   b.d_vals = vals;
   b.cap = (int64_t)n * L;
   b.stream = st;
+  b.profile = s->profile;
+  if (s->profile) profile_reset();
   SC_TRY(code_batch_f32(*s->ctx, b));
   // 4. A and B
   if (dA || dB) {
@@ -294,6 +297,12 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   // 5. next minibatch
   dl_advance_kernel<<<1, 1, 0, st>>>(d_iter);
   SC_CUDA(cudaGetLastError());
+  return SC_OK;
+}
+
+sc_status sc_dl_profile(sc_dl* s, int on) {
+  if (!s) return fail(SC_ERR_INVALID_ARG, "dictionary learning: null argument");
+  s->profile = on != 0;
   return SC_OK;
 }
 

@@ -224,6 +224,7 @@ struct Prof {
 };
 
 static void prof_reset() { memset(&g_prof, 0, sizeof(g_prof)); }
+void profile_reset() { prof_reset(); }
 
 // Blocks of the refinement pass for active sets beyond 32 atoms.
 constexpr int kRefineBigGrid = 32;
@@ -1031,6 +1032,7 @@ sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b) {
   }
   Prof pr;
   pr.st = st;
+  pr.on = b.profile;
   return run_pipeline<float>(c, st, p, b.G, nullptr, d_capflag, pr);
 }
 

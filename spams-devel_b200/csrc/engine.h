@@ -102,7 +102,9 @@ struct BatchDesc {
   float* d_vals = nullptr;
   int64_t cap = 0;
   cudaStream_t stream = nullptr;  // the stream to enqueue on (NULL: the legacy default stream)
+  bool profile = false;  // per-stage device times into the thread's sc_profile (synchronises)
 };
+void profile_reset();
 sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b);
 sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz);
 int pad_atoms(int K);

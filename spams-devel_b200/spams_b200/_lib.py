@@ -35,6 +35,7 @@ EXPORTS = (
     "sc_server_create", "sc_server_destroy", "sc_server_add_dictionary_f32",
     "sc_server_remove_dictionary", "sc_server_submit", "sc_server_wait", "sc_server_replay",
     "sc_server_stats_get", "sc_dl_create", "sc_dl_destroy", "sc_dl_step_f32", "sc_dl_codes",
+    "sc_dl_profile",
 )
 
 SC_REQ_OMP, SC_REQ_LASSO = 0, 1
@@ -150,6 +151,7 @@ def lib() -> C.CDLL:
         "sc_dl_destroy": (i32, [p]),
         "sc_dl_step_f32": (i32, [p, p, p, i64, p, p, p, p, f, f, p]),
         "sc_dl_codes": (i32, [p, C.POINTER(p), C.POINTER(p), C.POINTER(p)]),
+        "sc_dl_profile": (i32, [p, i32]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)

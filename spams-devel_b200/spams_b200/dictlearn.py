@@ -86,6 +86,11 @@ class MinibatchStep:
             self._h, vp(D), vp(X), int(X.shape[1]), vp(perm), vp(it), vp(A), vp(B),
             float(beta), float(gamma), C.c_void_p(s.cuda_stream)))
 
+    def profile(self, on: bool = True) -> None:
+        """Record the coding stages' device times of later (eager) steps, read
+        with spams_b200.last_profile()."""
+        _lib.check(_lib.lib().sc_dl_profile(self._h, int(bool(on))))
+
     def codes(self):
         """Copies of the last step's codes as CUDA tensors (colptr, rows, vals)."""
         import torch
