@@ -80,8 +80,18 @@ typedef struct {
   int refine;     /* > 0: refine the final single-precision coefficients in
                      FP64 on their active sets (from D, X and the Gram);
                      default off */
-  int reserved[4];
+  int kernel;     /* SC_KERNEL_*: which coding kernels may run; default
+                     SC_KERNEL_AUTO (timed once per shape, then cached).
+                     Every choice gives the same results. */
+  int reserved[3];
 } sc_options;
+
+/* Coding kernels: one warp per signal (up to 1024 atoms) or one CTA of
+ * Kp / 512 warps per signal (Kp, the padded atom count, a multiple of 512).
+ * SC_KERNEL_AUTO lets the engine time the admissible ones on the first call
+ * of each shape (set SC_AUTOTUNE=0 in the environment for the static rule:
+ * warp up to 1024 atoms, CTA beyond). */
+enum { SC_KERNEL_AUTO = 0, SC_KERNEL_WARP = 1, SC_KERNEL_CTA = 2 };
 
 /* What the calling thread's last coding call did on the device.  Stage times
  * are filled only when that call ran with sc_options.profile set. */
@@ -253,6 +263,7 @@ typedef struct {
   double busy_s;                /* wall time with at least one launch in flight */
   int64_t peak_device_bytes;    /* high-water mark of the admission count */
   double mean_batch_requests;   /* requests merged per launch */
+  char last_error[256];         /* message of the last failed request ("" if none) */
 } sc_server_stats;
 
 sc_status sc_server_create(int device, int64_t hbm_budget_bytes, int slots,

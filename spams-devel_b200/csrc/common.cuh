@@ -194,4 +194,25 @@ inline cudaError_t fill_grid(Kern k, int threads, size_t smem, int* grid) {
   return cudaSuccess;
 }
 
+// Lets kernel `k` launch with `smem` bytes of dynamic shared memory.  The
+// function attribute is process-wide, not per launch: it is always set to the
+// device's full opt-in size (less the kernel's static shared memory), the
+// same value from every caller, so that a thread launching this kernel with a
+// large size never races with another thread lowering the limit for a smaller
+// one.  Also prefers the largest shared-memory carveout.
+template <typename Kern>
+inline cudaError_t allow_smem(Kern k, size_t smem) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)k);
+  if (e != cudaSuccess) return e;
+  const int limit = optin - (int)fa.sharedSizeBytes;
+  if (smem > (size_t)limit) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 }  // namespace sc

@@ -11,8 +11,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -234,33 +236,30 @@ constexpr int kWarpMaxKp = 1024;
 constexpr int kCtaMaxKp = 4096;
 
 // ---------------------------------------------------------------------------
-// launch shapes
+// launch shapes and their autotuner
+//
+// A signal is coded either by one warp (Kp <= 1024; its correlations in that
+// warp's registers) or by one CTA of Kp / 512 warps (Kp a multiple of 512).
+// Both run the same arithmetic in the same order, so they give the same bits;
+// they differ in speed: the warp kernel packs more signals per SM, the CTA
+// kernel holds larger active sets in shared memory and codes each signal
+// with more threads (lower latency when the batch is small or the active
+// sets outgrow the warp's capacity and take the overflow rerun).  The first
+// call of each (algorithm, precision, Kp, L, batch-size class) times every
+// candidate on its first chunk and keeps the fastest; SC_AUTOTUNE=0 in the
+// environment selects the static rule instead (warp up to 1024 atoms).
 struct Shape {
-  bool cta;   // one CTA per signal (Kp > kWarpMaxKp)
+  bool cta;   // one CTA per signal
   int Lcap;   // active-set capacity in shared memory
-  int wpb;    // warps per block (warp kernels)
+  int wpb;    // warps per block (warp kernels) / per signal (CTA kernels)
   int grid;   // persistent blocks (0: filled by the CTA launcher)
 };
 
 template <typename T>
-static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
+static Shape warp_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap) {
   Shape s;
-  s.cta = Kp > kWarpMaxKp;
-  if (s.cta) {
-    // the small state is per CTA, so it can hold more atoms; keep two CTAs
-    // per SM within the shared-memory budget
-    s.wpb = Kp / 512;
-    s.grid = 0;
-    auto bytes = [&](int lc) {
-      return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
-    };
-    s.Lcap = std::max(1, std::min(L, 80));
-    while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
-                           2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
-      s.Lcap -= 16;
-    return s;
-  }
-  s.Lcap = std::max(1, std::min(L, 32));
+  s.cta = false;
+  s.Lcap = std::max(1, std::min(L, cap));
   s.wpb = 8;
   const size_t per_warp = lars ? lars_state_bytes(Kp, s.Lcap, sizeof(T))
                                : omp_state_bytes(Kp, s.Lcap, sizeof(T));
@@ -272,6 +271,64 @@ static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
   bps = std::max(1, std::min(bps, 64 / s.wpb));
   s.grid = c.num_sms * bps;
   return s;
+}
+
+template <typename T>
+static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
+  Shape s;
+  s.cta = true;
+  s.wpb = Kp / 512;
+  s.grid = 0;
+  // the small state is per CTA, so it can hold more atoms; keep two CTAs per
+  // SM within the shared-memory budget
+  auto bytes = [&](int lc) {
+    return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
+  };
+  s.Lcap = std::max(1, std::min(L, 80));
+  while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
+                         2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
+    s.Lcap -= 16;
+  return s;
+}
+
+// The static rule: warp kernel up to kWarpMaxKp atoms, CTA kernel beyond.
+template <typename T>
+static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
+  return Kp > kWarpMaxKp ? cta_shape<T>(c, lars, Kp, L) : warp_shape<T>(c, lars, Kp, L, 32);
+}
+
+// Every shape the layout Kp admits (the first one is the static rule's);
+// `kernel` (SC_KERNEL_*) keeps only one family.
+template <typename T>
+static std::vector<Shape> shape_candidates(const DeviceCtx& c, bool lars, int Kp, int L,
+                                           int kernel) {
+  std::vector<Shape> v;
+  const bool warp_ok = Kp <= kWarpMaxKp, cta_ok = Kp % 512 == 0 && Kp / 512 <= 8;
+  if (warp_ok && kernel != SC_KERNEL_CTA) {
+    v.push_back(warp_shape<T>(c, lars, Kp, L, 32));
+    if (L > 32) v.push_back(warp_shape<T>(c, lars, Kp, L, 64));
+  }
+  if (cta_ok && kernel != SC_KERNEL_WARP) v.push_back(cta_shape<T>(c, lars, Kp, L));
+  if (v.empty()) v.push_back(pick_shape<T>(c, lars, Kp, L));
+  return v;
+}
+
+struct TuneKey {
+  int lars, dbl, Kp, L, nclass, kernel;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(lars, dbl, Kp, L, nclass, kernel) <
+           std::tie(o.lars, o.dbl, o.Kp, o.L, o.nclass, o.kernel);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, int> g_tune;  // key -> index into shape_candidates
+
+static bool autotune_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SC_AUTOTUNE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 // ---------------------------------------------------------------------------
@@ -299,6 +356,7 @@ struct Problem {
   bool tc = false;
   bool refine = false;            // FP64 refinement of the final coefficients
   bool ols = false;               // least-squares refit on the final support (lasso ols)
+  int kernel = SC_KERNEL_AUTO;    // SC_KERNEL_*: kernel family (AUTO: tuned)
   const void* dDsplit = nullptr;  // Dhi (mp x K bf16) followed by Dlo
   int mp = 0;                     // m rounded up to the 64-element k-block
   int* d_tc_err = nullptr;
@@ -345,7 +403,7 @@ template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
-  const Shape shp = pick_shape<T>(c, p.lars, Kp, p.L);
+  const std::vector<Shape> cands = shape_candidates<T>(c, p.lars, Kp, p.L, p.kernel);
   const bool piped = sink && p.hX;
   const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
@@ -388,16 +446,21 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_TRY(sink->init(p.n));
   }
   // overflow pass: state in global slabs with capacity L (per warp, or per
-  // CTA for the CTA-per-signal kernels)
-  const int ovf_wpb = shp.cta ? 1 : 4;
-  const size_t ovf_per_warp =
-      shp.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
-              : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
-  int ovf_grid = shp.cta ? 2 * c.num_sms : c.num_sms;
-  while (ovf_grid > 1 && (size_t)ovf_grid * ovf_wpb * ovf_per_warp > ((size_t)256 << 20))
-    ovf_grid >>= 1;
-  const bool may_overflow = shp.Lcap < p.L;
-  if (may_overflow) SC_TRY(c.gstate.reserve((size_t)ovf_grid * ovf_wpb * ovf_per_warp));
+  // CTA for the CTA-per-signal kernels), at most 256 MiB
+  struct Ovf { int wpb, grid; size_t bytes; };
+  auto ovf_plan = [&](const Shape& sh) {
+    Ovf o;
+    o.wpb = sh.cta ? 1 : 4;
+    const size_t per =
+        sh.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
+               : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
+    o.grid = sh.cta ? 2 * c.num_sms : c.num_sms;
+    while (o.grid > 1 && (size_t)o.grid * o.wpb * per > ((size_t)256 << 20)) o.grid >>= 1;
+    o.bytes = (size_t)o.grid * o.wpb * per;
+    return o;
+  };
+  for (const Shape& sh : cands)
+    if (sh.Lcap < p.L) SC_TRY(c.gstate.reserve(ovf_plan(sh).bytes));
 
   unsigned* d_counter = misc_at<unsigned>(c.misc, MISC_COUNTERS);
   int* d_ovf_count = misc_at<int>(c.misc, MISC_OVF_COUNT);
@@ -450,6 +513,56 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     return SC_OK;
   };
 
+  // kernel family: a single candidate, the cached choice of an earlier call,
+  // the static rule, or timed on the first chunk (tune)
+  int chosen = cands.size() == 1 ? 0 : -1;
+  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, p.L, 0, p.kernel};
+  {
+    int64_t c0 = std::min<int64_t>(nc, p.n), cls = 0;
+    while (c0 > 1) { c0 >>= 1; ++cls; }
+    key.nclass = (int)cls;
+  }
+  if (chosen < 0 && !autotune_enabled()) chosen = 0;
+  if (chosen < 0) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end() && it->second < (int)cands.size()) chosen = it->second;
+  }
+  auto tune = [&](int64_t cn, auto& code, int& out) -> sc_status {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    SC_CUDA(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {  // no timing inside a graph capture
+      out = 0;
+      return SC_OK;
+    }
+    const int64_t sample = std::min<int64_t>(cn, 16384);
+    cudaEvent_t e0, e1;
+    SC_CUDA(cudaEventCreate(&e0));
+    SC_CUDA(cudaEventCreate(&e1));
+    int best = 0;
+    float best_ms = 0;
+    sc_status stt = SC_OK;
+    for (size_t i = 0; i < cands.size() && stt == SC_OK; ++i) {
+      stt = code(cands[i], std::min<int64_t>(sample, 64), false);  // module load, attributes
+      if (stt != SC_OK) break;
+      cudaEventRecord(e0, st);
+      stt = code(cands[i], sample, false);
+      cudaEventRecord(e1, st);
+      if (stt != SC_OK) break;
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (i == 0 || ms < best_ms) { best = (int)i; best_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stt != SC_OK) return stt;
+    out = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    return SC_OK;
+  };
+
   if (piped && nchunks > 0) {
     SC_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.last_use, 0));
     SC_TRY(issue_h2d(0));
@@ -494,57 +607,68 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       pr.launches(2);
     }
     // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
-    SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
-    pr.mark(ST_CODE);
     int* cnt = reinterpret_cast<int*>(c.cnt.ptr);
     int* sind = reinterpret_cast<int*>(c.slab_ind.ptr);
     T* sval = reinterpret_cast<T*>(c.slab_val.ptr);
     int64_t* ovf_list = reinterpret_cast<int64_t*>(c.ovf_list.ptr);
     T* path = start == 0 ? p.d_path : nullptr;
-    if (p.lars) {
-      LarsArgs<T> a{};
-      a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
-      a.Lcap = shp.Lcap; a.mode = p.mode; a.constraint = p.lambda1; a.pos = p.pos;
-      a.vConstraint = p.dLam1 ? p.dLam1 + start : nullptr;
-      a.length_path = p.length_path; a.n_jobs = (int)cn; a.n_jobs_dev = nullptr;
-      a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
-      a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
-      a.gstate = nullptr; a.path = path; a.steps = d_steps;
-      a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
-      if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
-      else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
-      pr.launches(1);
-      if (may_overflow) {
-        pr.launches(1);
-        a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
-        a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
-        a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
-        if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ovf_grid, st));
-        else SC_CUDA(launch_lars<T>(a, ovf_grid, ovf_wpb, st));
+    auto code = [&](const Shape& shp, int64_t jobs, bool final_run) -> sc_status {
+      SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
+      const bool may_overflow = shp.Lcap < p.L;
+      const Ovf ov = ovf_plan(shp);
+      if (p.lars) {
+        LarsArgs<T> a{};
+        a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
+        a.Lcap = shp.Lcap; a.mode = p.mode; a.constraint = p.lambda1; a.pos = p.pos;
+        a.vConstraint = p.dLam1 ? p.dLam1 + start : nullptr;
+        a.length_path = p.length_path; a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr;
+        a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
+        a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
+        a.gstate = nullptr; a.path = final_run ? path : nullptr;
+        a.steps = final_run ? d_steps : nullptr;
+        a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
+        if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
+        else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
+        if (final_run) pr.launches(1);
+        if (may_overflow) {
+          if (final_run) pr.launches(1);
+          a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
+          a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
+          a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
+          else SC_CUDA(launch_lars<T>(a, ov.grid, ov.wpb, st));
+        }
+      } else {
+        OmpArgs<T> a{};
+        a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
+        a.Lcap = shp.Lcap; a.eps = p.eps; a.lambda = p.lambda; a.Lsig = p.Lsig;
+        a.vL = p.dLv ? p.dLv + start : nullptr;
+        a.vEps = p.dEps ? p.dEps + start : nullptr;
+        a.vLambda = p.dLam ? p.dLam + start : nullptr;
+        a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
+        a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
+        a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
+        a.path = final_run ? path : nullptr;
+        a.steps = final_run ? d_steps : nullptr;
+        if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, shp.grid, st));
+        else SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
+        if (final_run) pr.launches(1);
+        if (may_overflow) {
+          if (final_run) pr.launches(1);
+          a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
+          a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
+          a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, ov.grid, st));
+          else SC_CUDA(launch_omp<T>(a, ov.grid, ov.wpb, st));
+        }
       }
-    } else {
-      OmpArgs<T> a{};
-      a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
-      a.Lcap = shp.Lcap; a.eps = p.eps; a.lambda = p.lambda; a.Lsig = p.Lsig;
-      a.vL = p.dLv ? p.dLv + start : nullptr;
-      a.vEps = p.dEps ? p.dEps + start : nullptr;
-      a.vLambda = p.dLam ? p.dLam + start : nullptr;
-      a.n_jobs = (int)cn; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
-      a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
-      a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
-      a.path = path; a.steps = d_steps;
-      if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, shp.grid, st));
-      else SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
-      pr.launches(1);
-      if (may_overflow) {
-        pr.launches(1);
-        a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
-        a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
-        a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
-        if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, ovf_grid, st));
-        else SC_CUDA(launch_omp<T>(a, ovf_grid, ovf_wpb, st));
-      }
-    }
+      return SC_OK;
+    };
+    if (chosen < 0) SC_TRY(tune(cn, code, chosen));
+    const Shape& shp = cands[(size_t)chosen];
+    const bool may_overflow = shp.Lcap < p.L;
+    pr.mark(ST_CODE);
+    SC_TRY(code(shp, cn, true));
     // ---- double-precision solves on the final active sets: the ols
     // projection, or the refinement of single-precision codes
     if (p.ols || (p.refine && (p.dD || p.dDtX))) {
@@ -646,6 +770,16 @@ int pad_atoms(int K) {
   const int p = pad128(K);
   return p <= kWarpMaxKp ? p : ((K + 511) / 512) * 512;
 }
+// The layout for a forced kernel family: CTA kernels need Kp % 512 == 0.
+static int pad_atoms_for(int K, const sc_options* opt) {
+  return opt && opt->kernel == SC_KERNEL_CTA ? ((K + 511) / 512) * 512 : pad_atoms(K);
+}
+static sc_status check_kernel(int K, const sc_options* opt) {
+  if (opt && opt->kernel == SC_KERNEL_WARP && pad128(K) > kWarpMaxKp)
+    return fail(SC_ERR_UNSUPPORTED, "the warp-per-signal kernels take at most %d atoms (K=%d)",
+                kWarpMaxKp, K);
+  return SC_OK;
+}
 
 // Per-call device guard: serialises calls on one device and orders this
 // call's stream after the previous user of the shared workspaces.
@@ -663,6 +797,8 @@ struct CallGuard {
 // precision calls always compute in FP64 and ignore the field.
 template <typename T>
 static sc_status check_opts(const sc_options* opt) {
+  if (opt && (opt->kernel < SC_KERNEL_AUTO || opt->kernel > SC_KERNEL_CTA))
+    return fail(SC_ERR_INVALID_ARG, "unknown kernel choice %d", opt->kernel);
   if (!opt || !std::is_same<T, float>::value) return SC_OK;
   if (opt->precision != SC_PREC_FP32 && opt->precision != SC_PREC_BF16X3)
     return fail(SC_ERR_INVALID_ARG, "unknown precision mode %d", opt->precision);
@@ -745,6 +881,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   SC_TRY(check_atoms(K));
 
   SC_TRY(check_opts<T>(opt));
+  SC_TRY(check_kernel(K, opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
@@ -752,7 +889,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  const int Kp = pad_atoms(K);
+  const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -792,6 +929,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   HostSink<T> sink;
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
+  p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   SC_TRY(check_tc<T>(*c, st, p));
   if (path)
@@ -845,6 +983,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   SC_TRY(check_atoms(K));
 
   SC_TRY(check_opts<T>(opt));
+  SC_TRY(check_kernel(K, opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   CallGuard g(c, c->stream);
@@ -852,7 +991,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   Prof pr;
   pr.on = opt && opt->profile;
   pr.st = st;
-  const int Kp = pad_atoms(K);
+  const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   Problem<T> p;
   p.lars = true;
@@ -892,6 +1031,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   HostSink<T> sink;
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
+  p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   SC_TRY(check_tc<T>(*c, st, p));
   if (p.d_path)
@@ -930,6 +1070,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
   SC_TRY(check_atoms(K));
   SC_TRY(check_opts<T>(opt));
+  SC_TRY(check_kernel(K, opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
@@ -944,7 +1085,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
     SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
     return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
   }
-  const int Kp = pad_atoms(K);
+  const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
   pr.mark(ST_GRAM);
@@ -956,6 +1097,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
   if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
+  p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
@@ -971,6 +1113,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
     return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
   SC_TRY(check_atoms(K));
   SC_TRY(check_opts<T>(opt));
+  SC_TRY(check_kernel(K, opt));
   DeviceCtx* c = nullptr;
   SC_TRY(get_ctx(opt ? opt->device : 0, &c));
   cudaStream_t st = (cudaStream_t)stream;
@@ -987,7 +1130,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
     SC_CUDA(cudaMemsetAsync(d_colptr, 0, sizeof(int64_t) * (size_t)(n + 1), st));
     return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
   }
-  const int Kp = pad_atoms(K);
+  const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   pr.mark(ST_GRAM);
   SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));
@@ -998,6 +1141,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
   if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
+  p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
@@ -1018,6 +1162,7 @@ sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b) {
   p.dLv = b.dLv; p.dEps = b.dEps; p.dLam = b.dLam;
   p.d_colptr = b.d_colptr; p.d_rows = b.d_rows; p.d_vals = b.d_vals; p.cap = b.cap;
   p.refine = b.refine;
+  p.kernel = b.kernel;
   if (b.tc) {
     if (!b.dDsplit) return fail(SC_ERR_INVALID_ARG, "batch: BF16 products without the split dictionary");
     p.tc = true;

@@ -97,6 +97,7 @@ struct BatchDesc {
   const float* dEps = nullptr;
   const float* dLam = nullptr;
   bool tc = false, refine = false;
+  int kernel = SC_KERNEL_AUTO;
   int64_t* d_colptr = nullptr;
   int32_t* d_rows = nullptr;
   float* d_vals = nullptr;

@@ -405,9 +405,7 @@ template <typename T, int NV>
 static cudaError_t launch_nv(const LarsArgs<T>& a, int grid, int warps_per_block,
                              size_t smem, cudaStream_t st) {
   auto k = lars_kernel<T, NV>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, warps_per_block * 32, smem, st>>>(a);
   return cudaGetLastError();

@@ -8,7 +8,7 @@
 // candidates, the correlation update) runs on all warps; cross-warp
 // arg-minima go through a W-entry exchange.  Every thread derives the step
 // and the control flow from the same shared values, so they agree bitwise.
-// Used for Kp = 1024 .. 4096 (W = Kp / 512) and active-set capacities up to L.
+// Used for Kp = 512 .. 4096 (W = Kp / 512) and active-set capacities up to L.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -424,9 +424,7 @@ lars_cta_kernel(const LarsArgs<T> a) {
 template <typename T, int W>
 static cudaError_t launch_w(const LarsArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
   auto k = lars_cta_kernel<T, W>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
   if (e != cudaSuccess) return e;
@@ -448,6 +446,7 @@ cudaError_t launch_lars_cta(const LarsArgs<T>& a, int grid, cudaStream_t st) {
   if (a.Kp % 512 != 0) return cudaErrorInvalidValue;
   const size_t smem = lars_cta_smem_bytes<T>(a.Kp, a.Lcap, a.gstate != nullptr);
   switch (a.Kp / 512) {
+    case 1: return launch_w<T, 1>(a, grid, smem, st);
     case 2: return launch_w<T, 2>(a, grid, smem, st);
     case 3: return launch_w<T, 3>(a, grid, smem, st);
     case 4: return launch_w<T, 4>(a, grid, smem, st);

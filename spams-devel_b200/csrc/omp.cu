@@ -228,9 +228,7 @@ omp_kernel(const OmpArgs<T> a) {
 template <typename T, int NV>
 static cudaError_t launch_nv(const OmpArgs<T>& a, int grid, int wpb, size_t smem, cudaStream_t st) {
   auto k = omp_kernel<T, NV>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, wpb * 32, smem, st>>>(a);
   return cudaGetLastError();

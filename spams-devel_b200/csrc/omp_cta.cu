@@ -6,7 +6,7 @@
 // The inverse Cholesky factor and the selection bookkeeping sit once per CTA
 // and are updated by warp 0; every warp updates its rows with the new
 // orthogonal direction and proposes its best atom; a W-entry exchange picks
-// the first index of the largest score.  Used for Kp = 1024 .. 4096.
+// the first index of the largest score.  Used for Kp = 512 .. 4096.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -237,9 +237,7 @@ omp_cta_kernel(const OmpArgs<T> a) {
 template <typename T, int W>
 static cudaError_t launch_w(const OmpArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
   auto k = omp_cta_kernel<T, W>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
   if (e != cudaSuccess) return e;
@@ -261,6 +259,7 @@ cudaError_t launch_omp_cta(const OmpArgs<T>& a, int grid, cudaStream_t st) {
   if (a.Kp % 512 != 0) return cudaErrorInvalidValue;
   const size_t smem = omp_cta_smem_bytes<T>(a.Kp, a.Lcap, a.gstate != nullptr);
   switch (a.Kp / 512) {
+    case 1: return launch_w<T, 1>(a, grid, smem, st);
     case 2: return launch_w<T, 2>(a, grid, smem, st);
     case 3: return launch_w<T, 3>(a, grid, smem, st);
     case 4: return launch_w<T, 4>(a, grid, smem, st);

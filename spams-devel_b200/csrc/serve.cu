@@ -15,6 +15,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdarg>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -105,6 +106,7 @@ struct sc_server {
   // statistics (since the last reset)
   std::vector<double> lat;
   int64_t completed = 0, signals = 0, batches = 0, batch_reqs = 0, rejected = 0;
+  std::string last_err;
   size_t peak = 0;
   int active = 0;
   Clock::time_point busy_from;
@@ -128,6 +130,7 @@ void finish_request(sc_server* s, SrvReq* q, Clock::time_point now) {
     s->signals += q->r.n;
   } else {
     ++s->rejected;
+    s->last_err = q->err;
   }
   auto it = s->dicts.find(q->r.dict_id);
   if (it != s->dicts.end()) --it->second->users;
@@ -623,6 +626,7 @@ sc_status sc_server_stats_get(sc_server* s, int reset, sc_server_stats* out) {
   out->signals = s->signals;
   out->batches = s->batches;
   out->rejected = s->rejected;
+  snprintf(out->last_error, sizeof(out->last_error), "%s", s->last_err.c_str());
   out->lat_p50_ms = percentile(s->lat, 50);
   out->lat_p99_ms = percentile(s->lat, 99);
   double sum = 0, mx = 0;
@@ -641,6 +645,7 @@ sc_status sc_server_stats_get(sc_server* s, int reset, sc_server_stats* out) {
   if (reset) {
     s->lat.clear();
     s->completed = s->signals = s->batches = s->batch_reqs = s->rejected = 0;
+    s->last_err.clear();
     s->busy_s = 0;
     if (s->active > 0) s->busy_from = Clock::now();
     s->peak = s->reserved_total();

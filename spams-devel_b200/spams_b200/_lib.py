@@ -25,6 +25,7 @@ SC_ERR_UNSUPPORTED = 9
 
 SC_L1COEFFS, SC_L2ERROR, SC_PENALTY = 0, 1, 2
 SC_PREC_FP32, SC_PREC_BF16X3 = 0, 1
+SC_KERNEL_AUTO, SC_KERNEL_WARP, SC_KERNEL_CTA = 0, 1, 2
 
 # every entry point the header declares (checked by the CPU test suite)
 EXPORTS = (
@@ -56,7 +57,7 @@ class CscF64(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("profile", C.c_int),
-                ("refine", C.c_int), ("reserved", C.c_int * 4)]
+                ("refine", C.c_int), ("kernel", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class Profile(C.Structure):
@@ -81,10 +82,13 @@ class ServerStats(C.Structure):
                 ("rejected", C.c_int64), ("pending", C.c_int64),
                 ("lat_p50_ms", C.c_double), ("lat_p99_ms", C.c_double),
                 ("lat_mean_ms", C.c_double), ("lat_max_ms", C.c_double), ("busy_s", C.c_double),
-                ("peak_device_bytes", C.c_int64), ("mean_batch_requests", C.c_double)]
+                ("peak_device_bytes", C.c_int64), ("mean_batch_requests", C.c_double),
+                ("last_error", C.c_char * 256)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["last_error"] = self.last_error.decode(errors="replace")
+        return d
 
 
 class ScError(RuntimeError):

@@ -36,13 +36,19 @@ def _ptr(a: Optional[np.ndarray], ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+_KERNELS = {None: 0, "auto": 0, "warp": 1, "cta": 2}
+
+
 def _opts(precision: Optional[int], device: int, profile: bool = False,
-          refine: Optional[bool] = None) -> Options:
+          refine: Optional[bool] = None, kernel: Optional[str] = None) -> Options:
     o = Options()
     o.precision = SC_PREC_FP32 if precision is None else int(precision)
     o.device = int(device)
     o.profile = int(bool(profile))
     o.refine = 0 if refine is None else (1 if refine else -1)
+    if kernel not in _KERNELS:
+        raise ValueError("spams_b200: kernel must be 'auto', 'warp' or 'cta'")
+    o.kernel = _KERNELS[kernel]
     return o
 
 
@@ -112,7 +118,7 @@ def _vec(v, dtype, n: int):
 
 
 def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=-1,
-        precision=None, device=0, refine=None):
+        precision=None, device=0, refine=None, kernel=None):
     """Orthogonal Matching Pursuit of every column of X on D (unit-norm atoms).
 
     Mirrors spams.omp (swig/python/spams.py:167-198): L / eps / lambda1 are
@@ -134,7 +140,7 @@ def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=
     out = CscF64() if f64 else CscF32()
     ct = C.c_double if f64 else C.c_float
     fn = _lib.lib().sc_omp_f64 if f64 else _lib.lib().sc_omp_f32
-    o = _opts(precision, device, refine=refine)
+    o = _opts(precision, device, refine=refine, kernel=kernel)
     st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Lv, C.c_int32), nL, _ptr(ev, ct), nE,
             _ptr(lv, ct), nLa, numThreads, _ptr(path, ct), C.byref(o), C.byref(out))
     _raise(st)
@@ -144,7 +150,8 @@ def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=
 
 def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, lambda2=0.,
           mode=SC_PENALTY, pos=False, ols=False, numThreads=-1, max_length_path=-1,
-          verbose=False, cholesky=False, precision=None, device=0, refine=None):
+          verbose=False, cholesky=False, precision=None, device=0, refine=None,
+          kernel=None):
     """LARS-Lasso of every column of X (swig/python/spams.py:109-142).
 
     mode 0: ||a||_1 <= lambda1; 1: ||x - D a||^2 <= lambda1; 2 (default):
@@ -163,7 +170,7 @@ def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, 
     f64 = dt == np.float64
     ct = C.c_double if f64 else C.c_float
     out = CscF64() if f64 else CscF32()
-    o = _opts(precision, device, refine=refine)
+    o = _opts(precision, device, refine=refine, kernel=kernel)
     if Q is not None:
         Q = _fortran(Q, dt)
         q = _fortran(q, dt)
@@ -209,7 +216,7 @@ def _clamp_lasso_L(m: int, K: int, L: int, lambda1: float, lambda2: float, mode:
 
 def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
                  max_length_path=-1, stream=None, precision=None, out=None, sync=True,
-                 profile=False, refine=None):
+                 profile=False, refine=None, kernel=None):
     """LARS-Lasso with X (m x n) and D (m x K) as column-major float32 CUDA
     tensors (i.e. the .t() views of row-major n x m / K x m tensors, or any
     tensor whose column j is contiguous).  Returns (colptr, rows, vals, nnz)
@@ -229,7 +236,7 @@ def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
     colptr, rows, vals = out
     nnz = C.c_int64(0)
     s = stream if stream is not None else torch.cuda.current_stream(X.device)
-    o = _opts(precision, X.device.index or 0, profile, refine)
+    o = _opts(precision, X.device.index or 0, profile, refine, kernel)
     st = _lib.lib().sc_lasso_f32_dev(
         C.c_void_p(X.data_ptr()), m, n, C.c_void_p(D.data_ptr()), K, int(L), float(lambda1),
         float(lambda2), int(mode), int(bool(pos)), int(max_length_path),
@@ -241,7 +248,7 @@ def lasso_device(X, D, lambda1, L=-1, lambda2=0.0, mode=SC_PENALTY, pos=False,
 
 def omp_device(X, D, L=None, eps=None, lambda1=None, L_vec=None, eps_vec=None,
                lambda_vec=None, stream=None, precision=None, out=None, sync=True,
-               profile=False, refine=None):
+               profile=False, refine=None, kernel=None):
     """OMP with CUDA tensors (see lasso_device).  Scalars L / eps / lambda1
     follow the facade defaults; *_vec are optional per-signal CUDA tensors
     (int32 / float32) of n entries, with L then the maximum of L_vec."""
@@ -265,7 +272,7 @@ def omp_device(X, D, L=None, eps=None, lambda1=None, L_vec=None, eps_vec=None,
     colptr, rows, vals = out
     nnz = C.c_int64(0)
     s = stream if stream is not None else torch.cuda.current_stream(X.device)
-    o = _opts(precision, X.device.index or 0, profile, refine)
+    o = _opts(precision, X.device.index or 0, profile, refine, kernel)
 
     def vp(t):
         return C.c_void_p(t.data_ptr()) if t is not None else None

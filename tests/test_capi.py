@@ -94,3 +94,19 @@ def test_dictionaries_beyond_4096_atoms_are_rejected_before_the_device():
     with pytest.raises(spams_b200.ScError) as e:
         spams_b200.lasso(X, D, lambda1=0.1)
     assert e.value.status == _lib.SC_ERR_UNSUPPORTED
+
+
+def test_kernel_choice_is_validated():
+    X = np.asfortranarray(np.random.randn(8, 4).astype(np.float32))
+    D = np.asfortranarray(np.random.randn(8, 6).astype(np.float32))
+    with pytest.raises(ValueError, match="kernel must be"):
+        spams_b200.omp(X, D, L=2, kernel="block")
+    o = _lib.Options()
+    o.kernel = 7
+    out = _lib.CscF32()
+    fp = C.POINTER(C.c_float)
+    st = spams_b200.lib().sc_omp_f32(X.ctypes.data_as(fp), 8, 4, D.ctypes.data_as(fp), 6,
+                                     (C.c_int32 * 1)(2), 1, None, 0, None, 0, -1, None,
+                                     C.byref(o), C.byref(out))
+    assert st == _lib.SC_ERR_INVALID_ARG
+    assert "kernel" in _lib.last_error()

@@ -111,6 +111,34 @@ def test_device_memory_budget():
             srv.add_dictionary(2, np.asfortranarray(np.ones((512, 4096), np.float32)))
 
 
+def test_concurrent_slots_with_every_kernel_shape():
+    """Slots launch the same kernels with different shared-memory sizes at
+    the same time (OMP requests of different L, Lasso with large active sets,
+    large and small dictionaries): every request succeeds and equals the
+    direct call."""
+    cases = [(64, 256), (96, 1024), (128, 2048)]
+    dicts, data = [], []
+    for i, (m, K) in enumerate(cases):
+        D, X = _draw(m, K, 600, 100 + i, s=20)
+        dicts.append(D)
+        data.append(X)
+    with spams_b200.Server(hbm_budget=20e9, slots=4) as srv:
+        for i, D in enumerate(dicts):
+            srv.add_dictionary(i, D)
+        jobs = []
+        for rep in range(6):
+            for i, X in enumerate(data):
+                L = 4 + 9 * rep
+                jobs.append((i, X, "omp", dict(L=L)))
+                jobs.append((i, X, "lasso", dict(lambda1=0.3 / (rep + 1))))
+        tickets = [srv.submit(i, X, algo, **kw) for i, X, algo, kw in jobs]
+        outs = [srv.result(t) for t in tickets]
+        st = srv.stats()
+    assert st["rejected"] == 0, st["last_error"]
+    for (i, X, algo, kw), a in zip(jobs, outs):
+        _same(a, _direct(algo, X, dicts[i], kw))
+
+
 def test_remove_dictionary_and_timeouts():
     D, X = _draw(64, 256, 100, 5)
     srv = spams_b200.Server(hbm_budget=2e9, slots=1)
@@ -149,7 +177,8 @@ def test_replay_reports_latencies():
         srv.replay(recs, reqs["arrival_s"])
         wall = time.perf_counter() - t0
         st = srv.stats()
-    assert st["completed"] == len(recs) and st["rejected"] == 0 and st["pending"] == 0
+    assert st["rejected"] == 0, st["last_error"]
+    assert st["completed"] == len(recs) and st["pending"] == 0
     assert st["signals"] == int(np.sum(reqs["n"]))
     assert 0 < st["lat_p50_ms"] <= st["lat_p99_ms"] <= st["lat_max_ms"]
     assert wall >= float(reqs["arrival_s"][-1])
