@@ -222,6 +222,35 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
 sc_status sc_corr_bf16x3_noalloc_f32(const float* dD, int m, int K, const float* dX, int64_t n,
                                      float* dC, int ldc, void* stream);
 
+/* ---- Masked variants ---------------------------------------------------
+ * Each signal x_i comes with a row mask (column i of `mask`, m x n bytes,
+ * column-major, nonzero = observed row): the code of x_i is computed from its
+ * observed rows only, i.e. against the rows of D that the mask keeps.
+ *   sc_omp_mask_*    replaces _ompMask<T>   (cpp_library/spams.h:296-343;
+ *                    omp_mask, decomp/decomp.h:406-481): a mask with no
+ *                    observed row gives an empty column, a full mask the plain
+ *                    OMP code; otherwise the masked Gram gets a 1e-10 ridge and
+ *                    eps scales by the observed fraction.  path as sc_omp_*.
+ *   sc_lasso_mask_*  replaces _lassoMask<T> (cpp_library/spams.h:191-214;
+ *                    lasso_mask, decomp/decomp.h:1466-1561): ridge
+ *                    max(lambda2, 1e-10); PENALTY and L2ERROR constraints scale
+ *                    by the observed fraction; L clamped as in _lassoD; no path.
+ * Dictionaries up to 1024 atoms (SC_ERR_UNSUPPORTED beyond). */
+sc_status sc_omp_mask_f32(const float* X, int m, int64_t n, const float* D, int K,
+                          const uint8_t* mask, const int* L, int64_t nL, const float* eps,
+                          int64_t nEps, const float* lambda, int64_t nLambda, int numThreads,
+                          float* path, const sc_options* opt, sc_csc_f32* out);
+sc_status sc_omp_mask_f64(const double* X, int m, int64_t n, const double* D, int K,
+                          const uint8_t* mask, const int* L, int64_t nL, const double* eps,
+                          int64_t nEps, const double* lambda, int64_t nLambda, int numThreads,
+                          double* path, const sc_options* opt, sc_csc_f64* out);
+sc_status sc_lasso_mask_f32(const float* X, int m, int64_t n, const float* D, int K,
+                            const uint8_t* mask, int L, float lambda1, float lambda2, int mode,
+                            int pos, int numThreads, const sc_options* opt, sc_csc_f32* out);
+sc_status sc_lasso_mask_f64(const double* X, int m, int64_t n, const double* D, int K,
+                            const uint8_t* mask, int L, double lambda1, double lambda2, int mode,
+                            int pos, int numThreads, const sc_options* opt, sc_csc_f64* out);
+
 /* ---- Serving: a request loop over resident dictionaries -----------------
  * No counterpart in the reference (each SPAMS call is synchronous and brings
  * its own dictionary).  A server keeps dictionaries resident on one GPU (D,

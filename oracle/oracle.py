@@ -239,6 +239,107 @@ def orc_lasso(X, D, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, max_lengt
     return (a, path) if return_reg_path else a
 
 
+def _mask(B, m, n):
+    B = np.asarray(B)
+    if B.shape != (m, n):
+        raise ValueError("ompMask : Mash has non acceptable dimensions")
+    return np.asfortranarray(B != 0, dtype=np.uint8)
+
+
+def ref_omp_mask(X, D, B, L=None, eps=None, lambda1=None, numThreads=-1, return_reg_path=False):
+    """The reference _ompMask<T> (cpp_library/spams.h:296-343) on X, D, B."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X, D = _f(X, dt), _f(D, dt)
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask(B, m, n)
+
+    def vec(v, t):
+        if v is None:
+            return None, 0
+        a = np.ascontiguousarray(np.atleast_1d(np.asarray(v, dtype=t)).ravel())
+        return a, a.size
+    Lv, nL = vec(L, np.int32)
+    ev, nE = vec(eps, dt)
+    lv, nLa = vec(lambda1, dt)
+    path = np.zeros((K, min(m, K)), dtype=dt, order="F") if return_reg_path else None
+    lib = _ref_lib()
+    fn = lib.ref_omp_mask_f64 if dt == np.float64 else lib.ref_omp_mask_f32
+    out = _RefCsc()
+    fn(_p(X), C.c_int(m), C.c_int(n), _p(D), C.c_int(K), _p(Bm), _p(Lv), C.c_int(nL), _p(ev),
+       C.c_int(nE), _p(lv), C.c_int(nLa), C.c_int(numThreads), _p(path), C.byref(out))
+    a = _csc_out(out, dt)
+    return (a, path) if return_reg_path else a
+
+
+def ref_lasso_mask(X, D, B, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, numThreads=-1):
+    """The reference _lassoMask<T> (cpp_library/spams.h:191-214) on X, D, B."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X, D = _f(X, dt), _f(D, dt)
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask(B, m, n)
+    ct = C.c_double if dt == np.float64 else C.c_float
+    lib = _ref_lib()
+    fn = lib.ref_lasso_mask_f64 if dt == np.float64 else lib.ref_lasso_mask_f32
+    out = _RefCsc()
+    fn(_p(X), C.c_int(m), C.c_int(n), _p(D), C.c_int(K), _p(Bm), C.c_int(L), ct(lambda1),
+       ct(lambda2), C.c_int(mode), C.c_int(int(pos)), C.c_int(numThreads), C.byref(out))
+    return _csc_out(out, dt)
+
+
+def orc_omp_mask(X, D, B, L=None, eps=None, lambda1=None, return_reg_path=False):
+    """C restatement of _ompMask / omp_mask (same facade defaults)."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X, D = _f(X, dt), _f(D, dt)
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask(B, m, n)
+    if L is None and eps is None and lambda1 is None:
+        raise ValueError("omp : You should either provide L, eps or lambda")
+    Lv = np.atleast_1d(np.asarray(min(m, K) if L is None else L, np.int32)).ravel().copy()
+    ev = np.atleast_1d(np.asarray(0.0 if eps is None else eps, dt)).ravel().copy()
+    lv = np.atleast_1d(np.asarray(0.0 if lambda1 is None else lambda1, dt)).ravel().copy()
+    Ld = int(Lv.max()) if Lv.size > 1 else int(Lv[0])
+    if Ld <= 0:
+        a = ssp.csc_matrix((0, 0), dtype=dt)
+        return (a, np.zeros((K, min(m, K)), dt, order="F")) if return_reg_path else a
+    Lc = min(m, min(Ld, K))
+    vM = np.zeros(max(1, Lc * n), dt)
+    rM = np.full(max(1, Lc * n), -1, np.int32)
+    path = np.zeros((K, min(m, K)), dt, order="F") if return_reg_path else None
+    lib = _orc_lib()
+    fn = lib.orc_omp_mask_f64 if dt == np.float64 else lib.orc_omp_mask_f32
+    fn(_p(X), C.c_int(m), C.c_int64(n), _p(D), C.c_int(K), _p(Bm), _p(Lv), C.c_int(Lv.size),
+       _p(ev), C.c_int(ev.size), _p(lv), C.c_int(lv.size), _p(vM), _p(rM), _p(path))
+    a = _convert(vM, rM, Lc, n, K, dt)
+    return (a, path) if return_reg_path else a
+
+
+def orc_lasso_mask(X, D, B, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False):
+    """C restatement of _lassoMask / lasso_mask (including the reference's
+    L explicit zeros at row 0 for a column with no observed row)."""
+    dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
+    X, D = _f(X, dt), _f(D, dt)
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask(B, m, n)
+    lib = _orc_lib()
+    ct = C.c_double if dt == np.float64 else C.c_float
+    clamp = lib.orc_lasso_clamp_f64 if dt == np.float64 else lib.orc_lasso_clamp_f32
+    mlp = C.c_int(-1)
+    Lc = clamp(C.c_int(m), C.c_int(K), C.c_int(L), ct(lambda1), ct(lambda2), C.c_int(mode),
+               C.c_int(int(pos)), C.byref(mlp))
+    if Lc <= 0:
+        return ssp.csc_matrix((0, 0), dtype=dt)
+    vM = np.zeros(max(1, Lc * n), dt)
+    rM = np.zeros(max(1, Lc * n), np.int32)
+    fn = lib.orc_lasso_mask_f64 if dt == np.float64 else lib.orc_lasso_mask_f32
+    fn(_p(X), C.c_int(m), C.c_int64(n), _p(D), C.c_int(K), _p(Bm), C.c_int(Lc), ct(lambda1),
+       ct(lambda2), C.c_int(mode), C.c_int(int(pos)), _p(vM), _p(rM))
+    return _convert(vM, rM, Lc, n, K, dt)
+
+
 def ols_refit(A, X, D, ridge):
     """Least-squares fit of every column of X on its support in A, with the
     Gram matrix G = D^T D + ridge I in the precision of X (the ols projection

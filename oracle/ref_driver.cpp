@@ -12,6 +12,10 @@
 //                   (-> lasso2<T> decomp/decomp.h:1563-1646, coreLARS2 :1706-1915,
 //                    or lasso<T>/coreLARS when cholesky/ols is set)
 //   ref_lassoQq_* -> _lassoQq<T> cpp_library/spams.h:145-188
+//   ref_omp_mask_*   -> _ompMask<T>   cpp_library/spams.h:296-343 (omp_mask,
+//                       decomp/decomp.h:406-519)
+//   ref_lasso_mask_* -> _lassoMask<T> cpp_library/spams.h:191-214 (lasso_mask,
+//                       decomp/decomp.h:1466-1561)
 // Outputs are copied out of the reference's SpMatrix<T> (linalg/linalg.h:775-935)
 // into malloc'd CSC arrays released by ref_free().
 #include "cppspams.h"
@@ -129,7 +133,83 @@ static int run_lassoQq(const T* X, int m, int n, const T* Q, int K, const T* q,
   return 0;
 }
 
+template <typename T>
+static int run_omp_mask(const T* X, int m, int n, const T* D, int K, const uint8_t* B,
+                        const int* L, int nL, const T* eps, int nEps, const T* lambda,
+                        int nLambda, int numThreads, T* path, ref_csc* out) {
+  memset(out, 0, sizeof(*out));
+  Matrix<T> mX(const_cast<T*>(X), m, n);
+  Matrix<T> mD(const_cast<T*>(D), m, K);
+  Matrix<bool> mB(reinterpret_cast<bool*>(const_cast<uint8_t*>(B)), m, n);
+  int Ldummy = 0;
+  T edummy = 0, ldummy = 0;
+  Vector<int> vL(nL > 0 ? const_cast<int*>(L) : &Ldummy, nL > 0 ? nL : 1);
+  Vector<T> vE(nEps > 0 ? const_cast<T*>(eps) : &edummy, nEps > 0 ? nEps : 1);
+  Vector<T> vLa(nLambda > 0 ? const_cast<T*>(lambda) : &ldummy,
+                nLambda > 0 ? nLambda : 1);
+  Matrix<T>* p = NULL;
+  SpMatrix<T>* a = NULL;
+  try {
+    a = _ompMask<T>(&mX, &mD, &mB, &p, path != NULL, nL > 0, &vL, nEps > 0, &vE,
+                    nLambda > 0, &vLa, numThreads);
+  } catch (const char* e) {
+    strncpy(out->err, e, sizeof(out->err) - 1);
+    return 1;
+  }
+  copy_out(a, out);
+  if (path && p) memcpy(path, p->rawX(), sizeof(T) * p->m() * p->n());
+  delete a;
+  delete p;
+  return 0;
+}
+
+template <typename T>
+static int run_lasso_mask(const T* X, int m, int n, const T* D, int K, const uint8_t* B,
+                          int L, T lambda1, T lambda2, int mode, int pos, int numThreads,
+                          ref_csc* out) {
+  memset(out, 0, sizeof(*out));
+  Matrix<T> mX(const_cast<T*>(X), m, n);
+  Matrix<T> mD(const_cast<T*>(D), m, K);
+  Matrix<bool> mB(reinterpret_cast<bool*>(const_cast<uint8_t*>(B)), m, n);
+  SpMatrix<T>* a = NULL;
+  try {
+    a = _lassoMask<T>(&mX, &mD, &mB, L, lambda1, lambda2, (constraint_type)mode, pos != 0,
+                      numThreads, false);
+  } catch (const char* e) {
+    strncpy(out->err, e, sizeof(out->err) - 1);
+    return 1;
+  }
+  copy_out(a, out);
+  delete a;
+  return 0;
+}
+
 extern "C" {
+
+int ref_omp_mask_f64(const double* X, int m, int n, const double* D, int K, const uint8_t* B,
+                     const int* L, int nL, const double* eps, int nEps, const double* lambda,
+                     int nLambda, int numThreads, double* path, ref_csc* out) {
+  return run_omp_mask<double>(X, m, n, D, K, B, L, nL, eps, nEps, lambda, nLambda, numThreads,
+                              path, out);
+}
+int ref_omp_mask_f32(const float* X, int m, int n, const float* D, int K, const uint8_t* B,
+                     const int* L, int nL, const float* eps, int nEps, const float* lambda,
+                     int nLambda, int numThreads, float* path, ref_csc* out) {
+  return run_omp_mask<float>(X, m, n, D, K, B, L, nL, eps, nEps, lambda, nLambda, numThreads,
+                             path, out);
+}
+int ref_lasso_mask_f64(const double* X, int m, int n, const double* D, int K, const uint8_t* B,
+                       int L, double lambda1, double lambda2, int mode, int pos, int numThreads,
+                       ref_csc* out) {
+  return run_lasso_mask<double>(X, m, n, D, K, B, L, lambda1, lambda2, mode, pos, numThreads,
+                                out);
+}
+int ref_lasso_mask_f32(const float* X, int m, int n, const float* D, int K, const uint8_t* B,
+                       int L, float lambda1, float lambda2, int mode, int pos, int numThreads,
+                       ref_csc* out) {
+  return run_lasso_mask<float>(X, m, n, D, K, B, L, lambda1, lambda2, mode, pos, numThreads,
+                               out);
+}
 
 int ref_omp_f64(const double* X, int m, int n, const double* D, int K,
                 const int* L, int nL, const double* eps, int nEps,

@@ -386,6 +386,113 @@ void F(orc_lasso)(const T* X, int m, int64_t n, const T* D, int K, int L,
   free(G); free(DtR);
 }
 
+/* Vector::copyMask / Matrix::copyMask (linalg/linalg.h:4082-4107): the
+ * observed rows of x and of D, compacted; returns their number. */
+static int F(orc_copy_mask)(const T* D, int m, int K, const T* x, const unsigned char* b,
+                            T* Dm, T* xm) {
+  int count = 0;
+  for (int r = 0; r < m; ++r) if (b[r]) xm[count++] = x[r];
+  for (int k = 0; k < K; ++k) {
+    int p = 0;
+    for (int r = 0; r < m; ++r)
+      if (b[r]) Dm[(size_t)k * count + p++] = D[(size_t)k * m + r];
+  }
+  return count;
+}
+
+/* omp_mask<T> driver (decomp/decomp.h:406-519), facade defaults resolved as
+ * in orc_omp.  B: m x n bytes, nonzero = observed row.  A column with no
+ * observed row keeps ind = -1 (empty); a full mask codes with D^T D; otherwise
+ * the observed rows' Gram + 1e-10 I, eps scaled by count / m. */
+int F(orc_omp_mask)(const T* X, int m, int64_t n, const T* D, int K, const unsigned char* B,
+                    const int* Lv, int nL, const T* eps, int nEps, const T* lambda,
+                    int nLambda, T* vM, int* rM, T* path) {
+  int L = Lv[0];
+  if (nL > 1)
+    for (int64_t i = 1; i < n; ++i) if (Lv[i] > L) L = Lv[i];
+  if (L <= 0) return 0;
+  if (L > K) L = K;
+  if (L > m) L = m;
+  T* G = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* Gm = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* Rdn = (T*)malloc(sizeof(T) * (size_t)K);
+  T* Dm = (T*)malloc(sizeof(T) * (size_t)m * K);
+  T* xm = (T*)malloc(sizeof(T) * (size_t)m);
+  F(orc_gram)(D, m, K, 0, G);
+  for (int64_t i = 0; i < n; ++i) {
+    const T* x = X + (size_t)i * m;
+    const unsigned char* b = B + (size_t)i * m;
+    int* ind = rM + (size_t)i * L;
+    for (int j = 0; j < L; ++j) ind[j] = -1;
+    int count = 0;
+    for (int r = 0; r < m; ++r) count += b[r] != 0;
+    if (count == 0) continue;
+    const int Li = nL > 1 ? Lv[i] : Lv[0];
+    const T ei = nEps > 1 ? eps[i] : eps[0];
+    const T li = nLambda > 1 ? lambda[i] : lambda[0];
+    T* pth = (path && i == 0) ? path : NULL;
+    if (count == m) {
+      T normX = 0;
+      for (int r = 0; r < m; ++r) normX += x[r] * x[r];
+      F(orc_dtx)(D, m, K, x, Rdn);
+      F(orc_omp_signal)(G, K, Rdn, normX, L, Li, ei, li, ind, vM + (size_t)i * L, pth);
+    } else {
+      F(orc_copy_mask)(D, m, K, x, b, Dm, xm);
+      T normX = 0;
+      for (int r = 0; r < count; ++r) normX += xm[r] * xm[r];
+      F(orc_dtx)(Dm, count, K, xm, Rdn);
+      F(orc_gram)(Dm, count, K, (T)1e-10, Gm);
+      const T eps_mask = ei * (T)count / (T)m;
+      F(orc_omp_signal)(Gm, K, Rdn, normX, L, Li, eps_mask, li, ind, vM + (size_t)i * L, pth);
+    }
+  }
+  free(G); free(Gm); free(Rdn); free(Dm); free(xm);
+  return L;
+}
+
+/* lasso_mask<T> driver (decomp/decomp.h:1466-1561), L already clamped as in
+ * _lassoMask.  rM must come zero-filled (Matrix::resize): a column with no
+ * observed row is left untouched there, so convert turns it into L zero
+ * entries at row 0, as the reference does.  Full masks code with
+ * D^T D + ridge; others with the observed rows' Gram + ridge and, in PENALTY
+ * and L2ERROR modes, the constraint scaled by count / m; coreLARS2 runs with
+ * its default path length. */
+void F(orc_lasso_mask)(const T* X, int m, int64_t n, const T* D, int K, const unsigned char* B,
+                       int L, T lambda1, T lambda2, int mode, int pos, T* vM, int* rM) {
+  if (L <= 0) return;
+  const T ridge = lambda2 > (T)1e-10 ? lambda2 : (T)1e-10;
+  T* G = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* Gm = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* DtR = (T*)malloc(sizeof(T) * (size_t)K);
+  T* Dm = (T*)malloc(sizeof(T) * (size_t)m * K);
+  T* xm = (T*)malloc(sizeof(T) * (size_t)m);
+  F(orc_gram)(D, m, K, ridge, G);
+  for (int64_t i = 0; i < n; ++i) {
+    const T* x = X + (size_t)i * m;
+    const unsigned char* b = B + (size_t)i * m;
+    int count = 0;
+    for (int r = 0; r < m; ++r) count += b[r] != 0;
+    if (count == 0) continue;
+    if (count == m) {
+      T normX = 0;
+      for (int r = 0; r < m; ++r) normX += x[r] * x[r];
+      F(orc_dtx)(D, m, K, x, DtR);
+      F(orc_lars_signal)(G, K, DtR, normX, L, mode, lambda1, pos, -1, rM + (size_t)i * L,
+                         vM + (size_t)i * L, NULL);
+    } else {
+      F(orc_copy_mask)(D, m, K, x, b, Dm, xm);
+      const T cm = (mode == 2 || mode == 1) ? lambda1 * (T)count / (T)m : lambda1;
+      T normX = 0;
+      for (int r = 0; r < count; ++r) normX += xm[r] * xm[r];
+      F(orc_dtx)(Dm, count, K, xm, DtR);
+      F(orc_gram)(Dm, count, K, ridge, Gm);
+      F(orc_lars_signal)(Gm, K, DtR, normX, L, mode, cm, pos, -1, rM + (size_t)i * L,
+                         vM + (size_t)i * L, NULL);
+    }
+  }
+  free(G); free(Gm); free(DtR); free(Dm); free(xm);
+}
+
 #undef F
 #undef ORC_MIN
 #undef CAT

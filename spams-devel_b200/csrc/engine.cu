@@ -357,6 +357,12 @@ struct Problem {
   bool refine = false;            // FP64 refinement of the final coefficients
   bool ols = false;               // least-squares refit on the final support (lasso ols)
   int kernel = SC_KERNEL_AUTO;    // SC_KERNEL_*: kernel family (AUTO: tuned)
+  // masked variants (lasso_mask / omp_mask): host row mask m x n, the ridge of
+  // the masked Grams, and whether the Lasso constraint is scaled by the
+  // observed fraction (PENALTY / L2ERROR; OMP always scales eps)
+  const uint8_t* hmask = nullptr;
+  T mask_ridge = 0;
+  int mask_scale = 0;
   const void* dDsplit = nullptr;  // Dhi (mp x K bf16) followed by Dlo
   int mp = 0;                     // m rounded up to the 64-element k-block
   int* d_tc_err = nullptr;
@@ -404,7 +410,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
   const std::vector<Shape> cands = shape_candidates<T>(c, p.lars, Kp, p.L, p.kernel);
-  const bool piped = sink && p.hX;
+  const bool piped = sink && p.hX && !p.hmask;
   const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
   const size_t per_sig = (size_t)Kp * sizeof(T) + (size_t)p.L * (sizeof(T) + 4) + 64 +
@@ -461,6 +467,31 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   };
   for (const Shape& sh : cands)
     if (sh.Lcap < p.L) SC_TRY(c.gstate.reserve(ovf_plan(sh).bytes));
+  // masked variants: Dᵀ, the chunk's mask / classes / scaled parameters, and
+  // one m-vector of scratch per warp of the largest launch
+  MaskArgs<T> mk{};
+  if (p.hmask) {
+    mk.m = p.m;
+    mk.mpad = (p.m + 31) / 32 * 32;
+    mk.ridge = p.mask_ridge;
+    mk.D = p.dD;
+    SC_TRY(c.Dt.reserve((size_t)Kp * p.m * sizeof(T)));
+    SC_CUDA(launch_transpose_pad<T>(p.dD, p.m, p.K, Kp, reinterpret_cast<T*>(c.Dt.ptr), st));
+    mk.Dt = reinterpret_cast<const T*>(c.Dt.ptr);
+    SC_TRY(c.mask.reserve((size_t)nc * p.m));
+    SC_TRY(c.mflag.reserve((size_t)nc));
+    SC_TRY(c.mvec.reserve((size_t)nc * sizeof(T)));
+    size_t warps = 0;
+    for (const Shape& sh : cands) {
+      warps = std::max(warps, (size_t)sh.grid * sh.wpb);
+      const Ovf ov = ovf_plan(sh);
+      warps = std::max(warps, (size_t)ov.grid * ov.wpb);
+    }
+    SC_TRY(c.mwork.reserve(warps * mk.mpad * sizeof(T)));
+    mk.mask = reinterpret_cast<const uint8_t*>(c.mask.ptr);
+    mk.flag = reinterpret_cast<const int8_t*>(c.mflag.ptr);
+    mk.work = reinterpret_cast<T*>(c.mwork.ptr);
+  }
 
   unsigned* d_counter = misc_at<unsigned>(c.misc, MISC_COUNTERS);
   int* d_ovf_count = misc_at<int>(c.misc, MISC_OVF_COUNT);
@@ -586,6 +617,23 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     } else {
       xchunk = p.dX + (size_t)start * p.m;
     }
+    T* mvec = nullptr;
+    if (p.hmask) {
+      // masked signal, observation classes, parameters scaled by the observed fraction
+      SC_CUDA(cudaMemcpyAsync(c.mask.ptr, p.hmask + (size_t)start * p.m, (size_t)cn * p.m,
+                              cudaMemcpyHostToDevice, st));
+      mvec = reinterpret_cast<T*>(c.mvec.ptr);
+      if (p.lars)
+        SC_CUDA(launch_mask_prep<T>(const_cast<T*>(xchunk), p.m, cn,
+                                    reinterpret_cast<const uint8_t*>(c.mask.ptr),
+                                    reinterpret_cast<int8_t*>(c.mflag.ptr), nullptr, p.lambda1,
+                                    p.mask_scale, mvec, st));
+      else
+        SC_CUDA(launch_mask_prep<T>(const_cast<T*>(xchunk), p.m, cn,
+                                    reinterpret_cast<const uint8_t*>(c.mask.ptr),
+                                    reinterpret_cast<int8_t*>(c.mflag.ptr),
+                                    p.dEps ? p.dEps + start : nullptr, p.eps, 1, mvec, st));
+    }
     pr.mark(ST_NORMS);
     SC_CUDA(launch_colnorms<T>(xchunk, p.m, cn, norms, st));
     pr.mark(ST_CORR);
@@ -620,7 +668,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         LarsArgs<T> a{};
         a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
         a.Lcap = shp.Lcap; a.mode = p.mode; a.constraint = p.lambda1; a.pos = p.pos;
-        a.vConstraint = p.dLam1 ? p.dLam1 + start : nullptr;
+        a.vConstraint = mvec ? mvec : (p.dLam1 ? p.dLam1 + start : nullptr);
+        a.mk = mk;
         a.length_path = p.length_path; a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr;
         a.sig_list = nullptr; a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval;
         a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
@@ -643,8 +692,9 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.G = dG; a.DtX = dtx; a.norms = norms; a.K = p.K; a.Kp = Kp; a.L = p.L;
         a.Lcap = shp.Lcap; a.eps = p.eps; a.lambda = p.lambda; a.Lsig = p.Lsig;
         a.vL = p.dLv ? p.dLv + start : nullptr;
-        a.vEps = p.dEps ? p.dEps + start : nullptr;
+        a.vEps = mvec ? mvec : (p.dEps ? p.dEps + start : nullptr);
         a.vLambda = p.dLam ? p.dLam + start : nullptr;
+        a.mk = mk;
         a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
         a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
         a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
@@ -774,6 +824,15 @@ int pad_atoms(int K) {
 static int pad_atoms_for(int K, const sc_options* opt) {
   return opt && opt->kernel == SC_KERNEL_CTA ? ((K + 511) / 512) * 512 : pad_atoms(K);
 }
+// The masked variants run on the warp-per-signal kernels only.
+static sc_status check_mask(int K, const uint8_t* mask, const sc_options* opt) {
+  if (!mask) return SC_OK;
+  if (pad128(K) > kWarpMaxKp)
+    return fail(SC_ERR_UNSUPPORTED, "masked coding takes at most %d atoms (K=%d)", kWarpMaxKp, K);
+  if (opt && opt->kernel == SC_KERNEL_CTA)
+    return fail(SC_ERR_UNSUPPORTED, "masked coding runs on the warp-per-signal kernels only");
+  return SC_OK;
+}
 static sc_status check_kernel(int K, const sc_options* opt) {
   if (opt && opt->kernel == SC_KERNEL_WARP && pad128(K) > kWarpMaxKp)
     return fail(SC_ERR_UNSUPPORTED, "the warp-per-signal kernels take at most %d atoms (K=%d)",
@@ -851,7 +910,8 @@ sc_status check_atoms(int K) {
 template <typename T>
 static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const int* Lv,
                           int64_t nL, const T* eps, int64_t nEps, const T* lam, int64_t nLam,
-                          T* path, const sc_options* opt, typename CscOf<T>::type* out) {
+                          T* path, const sc_options* opt, typename CscOf<T>::type* out,
+                          const uint8_t* mask = nullptr) {
   if (!out) return fail(SC_ERR_INVALID_ARG, "omp : null output");
   memset(out, 0, sizeof(*out));
   if (m < 0 || n < 0 || K < 0) return fail(SC_ERR_INVALID_ARG, "omp : negative dimension");
@@ -879,6 +939,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   L = std::min(m, std::min(L, K));
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
   SC_TRY(check_atoms(K));
+  SC_TRY(check_mask(K, mask, opt));
 
   SC_TRY(check_opts<T>(opt));
   SC_TRY(check_kernel(K, opt));
@@ -930,6 +991,12 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  if (mask) {  // omp_mask: masked Grams get a 1e-10 ridge, eps scales (decomp/decomp.h:477-481)
+    p.hmask = mask;
+    p.mask_ridge = T(1e-10);
+    p.kernel = SC_KERNEL_WARP;
+    p.refine = false;
+  }
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   SC_TRY(check_tc<T>(*c, st, p));
   if (path)
@@ -957,7 +1024,7 @@ template <typename T>
 static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q, const T* q,
                             int K, int L, T lambda1, T lambda2, int mode, int pos, int ols,
                             int max_length_path, int cholesky, T* path, const sc_options* opt,
-                            typename CscOf<T>::type* out) {
+                            typename CscOf<T>::type* out, const uint8_t* mask = nullptr) {
   if (!out) return fail(SC_ERR_INVALID_ARG, "lasso : null output");
   memset(out, 0, sizeof(*out));
   if (m < 0 || n < 0 || K < 0) return fail(SC_ERR_INVALID_ARG, "lasso : negative dimension");
@@ -981,6 +1048,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);
   SC_TRY(check_atoms(K));
+  SC_TRY(check_mask(K, mask, opt));
 
   SC_TRY(check_opts<T>(opt));
   SC_TRY(check_kernel(K, opt));
@@ -1032,6 +1100,18 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  if (mask) {
+    // lasso_mask: ridge max(lambda2, 1e-10) on the masked Grams, PENALTY and
+    // L2ERROR constraints scaled by the observed fraction, coreLARS2's default
+    // path length 4 L (decomp/decomp.h:1520-1545)
+    p.hmask = mask;
+    p.mask_ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
+    p.mask_scale = (mode == SC_PENALTY || mode == SC_L2ERROR) ? 1 : 0;
+    p.length_path = 4 * L;
+    p.kernel = SC_KERNEL_WARP;
+    p.refine = false;
+    p.ols = false;
+  }
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
   SC_TRY(check_tc<T>(*c, st, p));
   if (p.d_path)
@@ -1275,6 +1355,49 @@ sc_status sc_lasso_f64(const double* X, int m, int64_t n, const double* D, int K
   prof_reset();
   return lasso_host<double>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos,
                             ols, max_length_path, cholesky, path, opt, out);
+}
+
+sc_status sc_omp_mask_f32(const float* X, int m, int64_t n, const float* D, int K,
+                          const uint8_t* mask, const int* L, int64_t nL, const float* eps,
+                          int64_t nEps, const float* lambda, int64_t nLambda, int numThreads,
+                          float* path, const sc_options* opt, sc_csc_f32* out) {
+  (void)numThreads;
+  prof_reset();
+  if (!mask && n > 0 && m > 0) return fail(SC_ERR_INVALID_ARG, "ompMask : null mask");
+  static const uint8_t none = 1;
+  return omp_host<float>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out,
+                         mask ? mask : &none);
+}
+sc_status sc_omp_mask_f64(const double* X, int m, int64_t n, const double* D, int K,
+                          const uint8_t* mask, const int* L, int64_t nL, const double* eps,
+                          int64_t nEps, const double* lambda, int64_t nLambda, int numThreads,
+                          double* path, const sc_options* opt, sc_csc_f64* out) {
+  (void)numThreads;
+  prof_reset();
+  if (!mask && n > 0 && m > 0) return fail(SC_ERR_INVALID_ARG, "ompMask : null mask");
+  static const uint8_t none = 1;
+  return omp_host<double>(X, m, n, D, K, L, nL, eps, nEps, lambda, nLambda, path, opt, out,
+                          mask ? mask : &none);
+}
+sc_status sc_lasso_mask_f32(const float* X, int m, int64_t n, const float* D, int K,
+                            const uint8_t* mask, int L, float lambda1, float lambda2, int mode,
+                            int pos, int numThreads, const sc_options* opt, sc_csc_f32* out) {
+  (void)numThreads;
+  prof_reset();
+  if (!mask && n > 0 && m > 0) return fail(SC_ERR_INVALID_ARG, "lassoMask : null mask");
+  static const uint8_t none = 1;
+  return lasso_host<float>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos, 0, -1,
+                           0, nullptr, opt, out, mask ? mask : &none);
+}
+sc_status sc_lasso_mask_f64(const double* X, int m, int64_t n, const double* D, int K,
+                            const uint8_t* mask, int L, double lambda1, double lambda2, int mode,
+                            int pos, int numThreads, const sc_options* opt, sc_csc_f64* out) {
+  (void)numThreads;
+  prof_reset();
+  if (!mask && n > 0 && m > 0) return fail(SC_ERR_INVALID_ARG, "lassoMask : null mask");
+  static const uint8_t none = 1;
+  return lasso_host<double>(X, m, n, D, nullptr, nullptr, K, L, lambda1, lambda2, mode, pos, 0,
+                            -1, 0, nullptr, opt, out, mask ? mask : &none);
 }
 
 sc_status sc_lasso_gram_f32(const float* X, int m, int64_t n, const float* Q, int K,

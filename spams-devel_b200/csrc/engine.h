@@ -59,10 +59,11 @@ struct DeviceCtx {
   sc_status pinned_cols(size_t bytes);
   Buf X, D, G, dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, gstate;
   Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
+  Buf mask, mflag, mvec, Dt, mwork;  // masked variants
   std::vector<Buf*> all_bufs() {
     return {&X, &D, &G, &dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc,
             &scan, &gstate, &ccolptr, &crows, &cvals, &path, &vecs, &xstage, &xsplit,
-            &dsplit, &level, &rlist, &rscratch};
+            &dsplit, &level, &rlist, &rscratch, &mask, &mflag, &mvec, &Dt, &mwork};
   }
 };
 

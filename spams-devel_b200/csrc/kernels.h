@@ -25,6 +25,24 @@ __host__ __device__ inline size_t omp_state_bytes(int Kp, int Lc, size_t esz) {
                  4 * (size_t)Lc);
 }
 
+// Row masks of the masked variants (lasso_mask / omp_mask, decomp/decomp.h:
+// 406-519, 1466-1561): a signal whose rows are all observed is coded as
+// usual; one with some observed rows is coded against the Gram of its
+// observed rows (D_mᵀ D_m + ridge I), whose entries the kernel forms on the
+// fly: G_m(a, b) as a masked dot product of two atoms, and G_m(:, A) u as
+// Dᵀ (mask ∘ (D_A u)).  Its correlations and ||x||^2 come from the masked
+// signal (rows outside the mask set to zero).
+template <typename T>
+struct MaskArgs {
+  const uint8_t* mask = nullptr;  // m x n chunk, column-major, nonzero = observed row
+  const int8_t* flag = nullptr;   // n: 0 no row observed (empty code), 1 some, 2 all
+  const T* D = nullptr;           // m x K column-major
+  const T* Dt = nullptr;          // Kp x m column-major: Dᵀ with zero rows past K
+  int m = 0, mpad = 0;
+  T ridge = 0;                    // ridge of the masked Grams
+  T* work = nullptr;              // one mpad-vector per warp of the launch (global)
+};
+
 template <typename T>
 struct LarsArgs {
   const T* G;          // Kp x Kp, ld Kp, ridge included, zero padded
@@ -51,6 +69,7 @@ struct LarsArgs {
   T* path;             // K x length_path for signal 0, or NULL
   unsigned long long* steps;  // if set: total homotopy steps are added here
   T* out_level;        // if set: n correlation levels of the final active sets
+  MaskArgs<T> mk;      // masked variant (mk.mask set), warp kernels only
 };
 
 template <typename T>
@@ -78,6 +97,7 @@ struct OmpArgs {
   T* gstate;
   T* path;             // K x L for signal 0, or NULL
   unsigned long long* steps;  // if set: total OMP steps are added here
+  MaskArgs<T> mk;      // masked variant (mk.mask set), warp kernels only
 };
 
 template <typename T>
@@ -105,6 +125,16 @@ template <typename T>
 size_t omp_cta_gstate_bytes(int Lc, int grid);
 template <typename T>
 int omp_max_warps_per_sm(int Kp);
+
+// ---- masked variants
+template <typename T>
+cudaError_t launch_transpose_pad(const T* D, int m, int K, int Kp, T* Dt, cudaStream_t st);
+// X (in place): unobserved rows zeroed; flag: 0 / 1 / 2 = none / some / all
+// rows observed; out = value * count / m when some rows are and `scale`,
+// value otherwise (value = vbase[j], or base when vbase is NULL).
+template <typename T>
+cudaError_t launch_mask_prep(T* X, int m, int64_t n, const uint8_t* mask, int8_t* flag,
+                             const T* vbase, T base, int scale, T* out, cudaStream_t st);
 
 // ---- dense products ------------------------------------------------------
 // C (Kp x n, ld ldc) = A^T B with A m x Ka (ld lda), B m x n (ld ldb),

@@ -21,6 +21,7 @@
 // a global scratch slab per warp.
 #include "common.cuh"
 #include "kernels.h"
+#include "masked.cuh"
 
 namespace sc {
 
@@ -52,7 +53,7 @@ __device__ __forceinline__ T dot_row(const T* __restrict__ row, const T* __restr
 
 // Single precision: three 8-warp blocks per SM (80 registers); double
 // precision keeps two so that its wider row state stays in registers.
-template <typename T, int NV>
+template <typename T, int NV, bool MASKED = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 lars_kernel(const LarsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -99,6 +100,11 @@ lars_kernel(const LarsArgs<T> a) {
     const int64_t sig = a.sig_list ? a.sig_list[job] : (int64_t)job;
     const T constraint = a.vConstraint ? a.vConstraint[sig] : a.constraint;
     T* path = (a.path && sig == 0) ? a.path : nullptr;
+    // masked variant: no row observed -> empty code; some -> the masked Gram
+    const int mflag = MASKED ? (int)a.mk.flag[sig] : 2;
+    const bool partial = MASKED && mflag == 1;
+    const uint8_t* mrow = MASKED ? a.mk.mask + (size_t)sig * a.mk.m : nullptr;
+    T* mw = MASKED ? a.mk.work + (size_t)(blockIdx.x * wpb + wib) * a.mk.mpad : nullptr;
 
     // ---- load D^T x and find the first atom
     const T* dtx = a.DtX + (size_t)sig * Kp;
@@ -126,7 +132,7 @@ lars_kernel(const LarsArgs<T> a) {
 
     int cnt = 0;
     bool overflow = false;
-    bool skip = L <= 0;
+    bool skip = L <= 0 || mflag == 0;
     if (!skip) {
       const T dc = sDtR[cur];
       if (mode == 2 && fabs(dc) < constraint) skip = true;
@@ -148,8 +154,15 @@ lars_kernel(const LarsArgs<T> a) {
           if (lane == own_lane(cur)) act |= 1u << own_bit(cur);
           ++cnt;
           __syncwarp();
-          const T* gcol = a.G + (size_t)cur * Kp;
-          for (int j = lane; j <= i; j += 32) sG[j] = gcol[sInd[j]];
+          if (partial) {
+            for (int j = 0; j <= i; ++j) {
+              const T g = masked_gram(a.mk, mrow, sInd[j], cur);
+              if (lane == 0) sG[j] = g;
+            }
+          } else {
+            const T* gcol = a.G + (size_t)cur * Kp;
+            for (int j = lane; j <= i; j += 32) sG[j] = gcol[sInd[j]];
+          }
           __syncwarp();
           if (i == 0) {
             if (lane == 0) sInv[0] = T(1) / sG[0];
@@ -206,12 +219,16 @@ lars_kernel(const LarsArgs<T> a) {
         for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int e = 0; e < 4; ++e) A[v][e] = 0;
+        if (partial) {
+          masked_gram_times<T, NV>(a.mk, mrow, mw, Kp, sInd, sU, 1, i + 1, A);
+        } else {
 #pragma unroll 4
-        for (int j = 0; j <= i; ++j) {
-          const T uj = sU[j];
-          const T* gc = a.G + (size_t)sInd[j] * Kp + lane * 4;
+          for (int j = 0; j <= i; ++j) {
+            const T uj = sU[j];
+            const T* gc = a.G + (size_t)sInd[j] * Kp + lane * 4;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
+            for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
+          }
         }
 
         // ---- joining steps: first minimum magnitude over the 2K candidates.
@@ -404,7 +421,7 @@ size_t lars_smem_per_warp(int Kp, int Lcap) { return lars_state_bytes(Kp, Lcap, 
 template <typename T, int NV>
 static cudaError_t launch_nv(const LarsArgs<T>& a, int grid, int warps_per_block,
                              size_t smem, cudaStream_t st) {
-  auto k = lars_kernel<T, NV>;
+  auto k = a.mk.mask ? lars_kernel<T, NV, true> : lars_kernel<T, NV, false>;
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, warps_per_block * 32, smem, st>>>(a);

@@ -17,10 +17,11 @@
 // Lane `l` owns rows r = 128 v + 4 l + e as in the LARS kernel.
 #include "common.cuh"
 #include "kernels.h"
+#include "masked.cuh"
 
 namespace sc {
 
-template <typename T, int NV>
+template <typename T, int NV, bool MASKED = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 omp_kernel(const OmpArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -58,6 +59,11 @@ omp_kernel(const OmpArgs<T> a) {
     const T lambda = a.vLambda ? a.vLambda[sig] : a.lambda;
     T normX = a.norms[sig];
     T* path = (a.path && sig == 0) ? a.path : nullptr;
+    // masked variant: no row observed -> empty code; some -> the masked Gram
+    const int mflag = MASKED ? (int)a.mk.flag[sig] : 2;
+    const bool partial = MASKED && mflag == 1;
+    const uint8_t* mrow = MASKED ? a.mk.mask + (size_t)sig * a.mk.m : nullptr;
+    T* mw = MASKED ? a.mk.work + (size_t)(blockIdx.x * wpb + wib) * a.mk.mpad : nullptr;
 
     // ---- load D^T x; norm = 1; first choice = first max |D^T x|
     const T* dtx = a.DtX + (size_t)sig * Kp;
@@ -85,7 +91,7 @@ omp_kernel(const OmpArgs<T> a) {
     int j = 0;
     bool overflow = false;
     uint32_t act = 0;
-    const bool started = !(normX <= eps || L <= 0);
+    const bool started = !(normX <= eps || L <= 0 || mflag == 0);
     if (started) {
       for (j = 0; j < L; ++j) {
         if (j >= Lc) { overflow = true; break; }
@@ -99,8 +105,15 @@ omp_kernel(const OmpArgs<T> a) {
         if (lane == 0) { sRUn[j] = RU; sInd[j] = c; }
         if (lane == ((c & 127) >> 2)) act |= 1u << (((c >> 7) << 2) | (c & 3));
         // g_l = G(c, ind_l), l < j
-        const T* gcol = a.G + (size_t)c * Kp;
-        for (int l = lane; l < j; l += 32) sGg[l] = gcol[sInd[l]];
+        if (partial) {
+          for (int l = 0; l < j; ++l) {
+            const T g = masked_gram(a.mk, mrow, sInd[l], c);
+            if (lane == 0) sGg[l] = g;
+          }
+        } else {
+          const T* gcol = a.G + (size_t)c * Kp;
+          for (int l = lane; l < j; l += 32) sGg[l] = gcol[sInd[l]];
+        }
         __syncwarp();
         // Undn(c, k) = sum_{l<=k} g_l Un(l, k), k < j
         for (int k = lane; k < j; k += 32) {
@@ -133,15 +146,19 @@ omp_kernel(const OmpArgs<T> a) {
         for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int e = 0; e < 4; ++e) A[v][e] = 0;
+        if (partial) {
+          masked_gram_times<T, NV>(a.mk, mrow, mw, Kp, sInd, sUn + j, ldu, j + 1, A);
+        } else {
 #pragma unroll 4
-        for (int l = 0; l <= j; ++l) {
-          const T ul = sUn[(size_t)l * ldu + j];
-          const T* gc = a.G + (size_t)sInd[l] * Kp + lane * 4;
+          for (int l = 0; l <= j; ++l) {
+            const T ul = sUn[(size_t)l * ldu + j];
+            const T* gc = a.G + (size_t)sInd[l] * Kp + lane * 4;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            const Vec4<T> g = ldg4(gc + v * 128);
+            for (int v = 0; v < NV; ++v) {
+              const Vec4<T> g = ldg4(gc + v * 128);
 #pragma unroll
-            for (int e = 0; e < 4; ++e) A[v][e] += g.v[e] * ul;
+              for (int e = 0; e < 4; ++e) A[v][e] += g.v[e] * ul;
+            }
           }
         }
         // ---- residual correlations, norms, scores; next choice (first index
@@ -227,7 +244,7 @@ omp_kernel(const OmpArgs<T> a) {
 
 template <typename T, int NV>
 static cudaError_t launch_nv(const OmpArgs<T>& a, int grid, int wpb, size_t smem, cudaStream_t st) {
-  auto k = omp_kernel<T, NV>;
+  auto k = a.mk.mask ? omp_kernel<T, NV, true> : omp_kernel<T, NV, false>;
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, wpb * 32, smem, st>>>(a);

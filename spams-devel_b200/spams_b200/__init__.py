@@ -15,7 +15,8 @@ learning.
 """
 from ._lib import (SC_L1COEFFS, SC_L2ERROR, SC_PENALTY, SC_PREC_BF16X3, SC_PREC_FP32,  # noqa: F401
                    ScError, device_count, last_error, last_profile, lib)
-from .api import corr_device, lasso, lasso_device, omp, omp_device  # noqa: F401
+from .api import (corr_device, lasso, lasso_device, lassoMask, omp, omp_device,  # noqa: F401
+                  ompMask)
 from .serve import Server, request  # noqa: F401
 from .dictlearn import MinibatchStep  # noqa: F401
 

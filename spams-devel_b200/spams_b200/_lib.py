@@ -36,7 +36,8 @@ EXPORTS = (
     "sc_server_create", "sc_server_destroy", "sc_server_add_dictionary_f32",
     "sc_server_remove_dictionary", "sc_server_submit", "sc_server_wait", "sc_server_replay",
     "sc_server_stats_get", "sc_dl_create", "sc_dl_destroy", "sc_dl_step_f32", "sc_dl_codes",
-    "sc_dl_profile",
+    "sc_dl_profile", "sc_omp_mask_f32", "sc_omp_mask_f64", "sc_lasso_mask_f32",
+    "sc_lasso_mask_f64",
 )
 
 SC_REQ_OMP, SC_REQ_LASSO = 0, 1
@@ -156,6 +157,14 @@ def lib() -> C.CDLL:
         "sc_dl_step_f32": (i32, [p, p, p, i64, p, p, p, p, f, f, p]),
         "sc_dl_codes": (i32, [p, C.POINTER(p), C.POINTER(p), C.POINTER(p)]),
         "sc_dl_profile": (i32, [p, i32]),
+        "sc_omp_mask_f32": (i32, [f32p, i32, i64, f32p, i32, C.POINTER(C.c_uint8), i32p, i64, f32p, i64, f32p,
+                                  i64, i32, f32p, opt, C.POINTER(CscF32)]),
+        "sc_omp_mask_f64": (i32, [f64p, i32, i64, f64p, i32, C.POINTER(C.c_uint8), i32p, i64, f64p, i64, f64p,
+                                  i64, i32, f64p, opt, C.POINTER(CscF64)]),
+        "sc_lasso_mask_f32": (i32, [f32p, i32, i64, f32p, i32, C.POINTER(C.c_uint8), i32, f, f, i32, i32, i32,
+                                    opt, C.POINTER(CscF32)]),
+        "sc_lasso_mask_f64": (i32, [f64p, i32, i64, f64p, i32, C.POINTER(C.c_uint8), i32, d, d, i32, i32, i32,
+                                    opt, C.POINTER(CscF64)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)

@@ -202,6 +202,73 @@ def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, 
     return (alpha, path) if return_reg_path else alpha
 
 
+def _mask_of(B, m: int, n: int, name: str) -> np.ndarray:
+    B = np.asarray(B)
+    if B.shape != (m, n):
+        raise ValueError(f"{name} : Mash has non acceptable dimensions")
+    return np.asfortranarray(B != 0, dtype=np.uint8)
+
+
+def ompMask(X, D, B, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=-1,
+            precision=None, device=0):
+    """OMP of every column of X on its observed rows (swig/python/spams.py:201-232).
+
+    B (m x n, boolean) marks the observed rows of each signal; a signal is
+    coded against the rows of D its mask keeps (eps scaled by the observed
+    fraction), an all-false column gives an empty code."""
+    dt = _dtype_of(np.asarray(X))
+    X = _fortran(X, dt)
+    D = _fortran(D, dt)
+    if X.ndim != 2 or D.ndim != 2 or X.shape[0] != D.shape[0]:
+        raise ValueError("ompMask : incompatible matrix dimensions")
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask_of(B, m, n, "ompMask")
+    if L is None and eps is None and lambda1 is None:
+        raise ValueError("omp : You should either provide L, eps or lambda")
+    Lv, nL = _vec(L, np.int32, n)
+    ev, nE = _vec(eps, dt, n)
+    lv, nLa = _vec(lambda1, dt, n)
+    path = np.zeros((K, min(m, K)), dtype=dt, order="F") if return_reg_path else None
+    f64 = dt == np.float64
+    out = CscF64() if f64 else CscF32()
+    ct = C.c_double if f64 else C.c_float
+    fn = _lib.lib().sc_omp_mask_f64 if f64 else _lib.lib().sc_omp_mask_f32
+    o = _opts(precision, device)
+    st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Bm, C.c_uint8), _ptr(Lv, C.c_int32), nL,
+            _ptr(ev, ct), nE, _ptr(lv, ct), nLa, numThreads, _ptr(path, ct), C.byref(o),
+            C.byref(out))
+    _raise(st)
+    alpha = _csc_from(out, f64)
+    return (alpha, path) if return_reg_path else alpha
+
+
+def lassoMask(X, D, B, L=-1, lambda1=None, lambda2=0., mode=SC_PENALTY, pos=False,
+              numThreads=-1, verbose=False, precision=None, device=0):
+    """LARS-Lasso of every column of X on its observed rows
+    (swig/python/spams.py:144-153): B (m x n, boolean) marks the observed rows;
+    PENALTY / L2ERROR constraints scale by the observed fraction."""
+    if lambda1 is None:
+        raise ValueError("lassoMask : lambda1 must be defined")
+    dt = _dtype_of(np.asarray(X))
+    X = _fortran(X, dt)
+    D = _fortran(D, dt)
+    if X.ndim != 2 or D.ndim != 2 or X.shape[0] != D.shape[0]:
+        raise ValueError("lassoMask : incompatible matrix dimensions")
+    m, n = X.shape
+    K = D.shape[1]
+    Bm = _mask_of(B, m, n, "lassoMask")
+    f64 = dt == np.float64
+    out = CscF64() if f64 else CscF32()
+    ct = C.c_double if f64 else C.c_float
+    fn = _lib.lib().sc_lasso_mask_f64 if f64 else _lib.lib().sc_lasso_mask_f32
+    o = _opts(precision, device)
+    st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Bm, C.c_uint8), int(L), float(lambda1),
+            float(lambda2), int(mode), int(bool(pos)), numThreads, C.byref(o), C.byref(out))
+    _raise(st)
+    return _csc_from(out, f64)
+
+
 # ---------------------------------------------------------------------------
 # device-resident front ends (torch CUDA tensors in and out)
 

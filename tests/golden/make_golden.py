@@ -76,6 +76,24 @@ def cases():
     Q = D.T @ D
     q = D.T @ X
     out.append(dict(name="lassoQq", algo="lassoQq", X=X, D=D, Q=Q, q=q, kw=dict(lambda1=0.1), path=False))
+    # masked variants: random observed rows (70 %), plus one fully observed,
+    # one unobserved and one mostly observed column.  ompMask gets L, eps and
+    # lambda explicitly: the reference facade points eps / lambda at an
+    # out-of-scope local when they are not given (cpp_library/spams.h:323-333)
+    r = rng(8)
+    D = W.gaussian_dictionary(40, 120, r)
+    X, _, _ = W.sparse_signals(D, 160, 6, 0.05, r)
+    B = r.random((40, 160)) < 0.7
+    B[:, 0] = True
+    B[:, 1] = False
+    B[:5, 2] = False
+    B = B.astype(np.uint8)
+    out.append(dict(name="omp_mask", algo="omp_mask", X=X, D=D, B=B,
+                    kw=dict(L=8, eps=0.02, lambda1=0.0), path=True))
+    out.append(dict(name="lasso_mask", algo="lasso_mask", X=X, D=D, B=B,
+                    kw=dict(lambda1=0.05), path=False))
+    out.append(dict(name="lasso_mask_l2err_pos", algo="lasso_mask", X=X, D=D, B=B,
+                    kw=dict(lambda1=0.3, mode=1, pos=True), path=False))
     return out
 
 
@@ -88,6 +106,10 @@ def run(case, dt):
             kw[k] = np.asarray(kw[k]).astype(np.float32).astype(dt)
     if case["algo"] == "omp":
         return O.ref_omp(X, D, return_reg_path=case["path"], **kw)
+    if case["algo"] == "omp_mask":
+        return O.ref_omp_mask(X, D, case["B"], return_reg_path=case["path"], **kw)
+    if case["algo"] == "lasso_mask":
+        return O.ref_lasso_mask(X, D, case["B"], **kw)
     if case["algo"] == "lassoQq":
         Q = case["Q"].astype(np.float32).astype(dt)
         q = case["q"].astype(np.float32).astype(dt)
@@ -105,6 +127,8 @@ def main():
             # per-signal float arrays were rounded to float32 for both runs;
             # scalars were passed as given
             rec["kw_" + k] = v.astype(np.float32) if (v.dtype.kind == "f" and v.ndim > 0) else v
+        if "B" in case:
+            rec["B"] = case["B"]
         if "Q" in case:
             rec["Q"] = case["Q"].astype(np.float32)
             rec["q"] = case["q"].astype(np.float32)

@@ -110,3 +110,17 @@ def test_kernel_choice_is_validated():
                                      C.byref(o), C.byref(out))
     assert st == _lib.SC_ERR_INVALID_ARG
     assert "kernel" in _lib.last_error()
+
+
+def test_mask_front_ends_check_arguments_without_a_device():
+    X = np.asfortranarray(np.random.randn(8, 4))
+    D = np.asfortranarray(np.random.randn(8, 6))
+    B = np.ones((8, 4), bool)
+    with pytest.raises(ValueError, match="non acceptable dimensions"):
+        spams_b200.ompMask(X, D, B[:, :3], L=2)
+    with pytest.raises(ValueError, match="either provide L, eps or lambda"):
+        spams_b200.ompMask(X, D, B)
+    with pytest.raises(ValueError, match="lambda1 must be defined"):
+        spams_b200.lassoMask(X, D, B)
+    with pytest.raises(ValueError, match="incompatible matrix dimensions"):
+        spams_b200.lassoMask(X, np.asfortranarray(np.random.randn(9, 6)), B, lambda1=0.1)

@@ -30,6 +30,12 @@ def _gpu_run(g, dt, **extra):
     path = "f64_path" in g
     if g["algo"] == "omp":
         return spams_b200.omp(X, D, return_reg_path=path, **kw)
+    if g["algo"] == "omp_mask":
+        return spams_b200.ompMask(X, D, g["B"], return_reg_path=path, **kw)
+    if g["algo"] == "lasso_mask":
+        a = spams_b200.lassoMask(X, D, g["B"], **kw).copy()
+        a.eliminate_zeros()  # as golden_csc does for the reference's output
+        return a
     if g["algo"] == "lassoQq":
         Q = g["Q"].astype(dt)
         q = g["q"].astype(dt)

@@ -15,6 +15,12 @@ def _orc_run(g, dt):
     path = f"f64_path" in g
     if g["algo"] == "omp":
         return O.orc_omp(X, D, return_reg_path=path, **kw)
+    if g["algo"] == "omp_mask":
+        return O.orc_omp_mask(X, D, g["B"], return_reg_path=path, **kw)
+    if g["algo"] == "lasso_mask":
+        a = O.orc_lasso_mask(X, D, g["B"], **kw).copy()
+        a.eliminate_zeros()
+        return a
     if g["algo"] == "lassoQq":
         # the restatement computes the products itself from D; Q, q in the
         # fixture are D^T D and D^T X of the same float32 data
