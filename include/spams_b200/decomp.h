@@ -58,6 +58,32 @@ inline sc_status call_lassoQq(const double* X, int m, int64_t n, const double* Q
                               int mlp, double* path, sc_csc_f64* out) {
   return sc_lasso_gram_f64(X, m, n, Q, K, q, L, l1, l2, mode, pos, -1, mlp, path, nullptr, out);
 }
+inline sc_status call_omp_mask(const float* X, int m, int64_t n, const float* D, int K,
+                               const bool* B, const int* L, int64_t nL, const float* e,
+                               int64_t nE, const float* la, int64_t nLa, float* path,
+                               sc_csc_f32* out) {
+  return sc_omp_mask_f32(X, m, n, D, K, reinterpret_cast<const uint8_t*>(B), L, nL, e, nE, la,
+                         nLa, -1, path, nullptr, out);
+}
+inline sc_status call_omp_mask(const double* X, int m, int64_t n, const double* D, int K,
+                               const bool* B, const int* L, int64_t nL, const double* e,
+                               int64_t nE, const double* la, int64_t nLa, double* path,
+                               sc_csc_f64* out) {
+  return sc_omp_mask_f64(X, m, n, D, K, reinterpret_cast<const uint8_t*>(B), L, nL, e, nE, la,
+                         nLa, -1, path, nullptr, out);
+}
+inline sc_status call_lasso_mask(const float* X, int m, int64_t n, const float* D, int K,
+                                 const bool* B, int L, float l1, float l2, int mode, int pos,
+                                 sc_csc_f32* out) {
+  return sc_lasso_mask_f32(X, m, n, D, K, reinterpret_cast<const uint8_t*>(B), L, l1, l2, mode,
+                           pos, -1, nullptr, out);
+}
+inline sc_status call_lasso_mask(const double* X, int m, int64_t n, const double* D, int K,
+                                 const bool* B, int L, double l1, double l2, int mode, int pos,
+                                 sc_csc_f64* out) {
+  return sc_lasso_mask_f64(X, m, n, D, K, reinterpret_cast<const uint8_t*>(B), L, l1, l2, mode,
+                           pos, -1, nullptr, out);
+}
 inline void release(sc_csc_f32* a) { sc_csc_free_f32(a); }
 inline void release(sc_csc_f64* a) { sc_csc_free_f64(a); }
 
@@ -180,6 +206,46 @@ void lasso(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha, int L,
     for (size_t c = 0; c < cols; ++c)
       memcpy(path->rawX() + c * path->m(), pbuf.data() + c * K, sizeof(T) * std::min<INTM>(K, path->m()));
   }
+}
+
+// decomp/decomp.h:406-519: each column coded from the rows its mask column
+// keeps (bool, one byte per entry as in the reference's Matrix<bool>).
+template <typename T>
+void omp_mask(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha,
+              const Matrix<bool>& mask, const int* L, const T* eps, const T* lambda,
+              const bool vecL = false, const bool vecEps = false, const bool vecLambda = false,
+              const int numThreads = -1, Matrix<T>* path = NULL) {
+  (void)numThreads;
+  namespace d = spams_b200_detail;
+  const INTM m = X.m(), n = X.n(), K = D.n();
+  const INTM pathL = std::min(m, K);
+  std::vector<T> pbuf(path ? (size_t)K * pathL : 0);
+  typename d::Csc<T>::type out;
+  d::check(d::call_omp_mask(X.X(), (int)m, n, D.X(), (int)K, mask.X(), L, vecL ? n : 1, eps,
+                            vecEps ? n : 1, lambda, vecLambda ? n : 1,
+                            path ? pbuf.data() : nullptr, &out));
+  d::adopt<T>(out, spalpha);
+  if (path) {
+    const size_t cols = std::min<size_t>((size_t)path->n(), (size_t)pathL);
+    for (size_t c = 0; c < cols; ++c)
+      memcpy(path->rawX() + c * path->m(), pbuf.data() + c * K, sizeof(T) * std::min<INTM>(K, path->m()));
+  }
+}
+
+// decomp/decomp.h:1466-1561 with L as the _lassoMask facade clamps it.  A
+// column with no observed row is empty here (the reference's CSC holds L
+// explicit zeros at row 0 for it, the same dense matrix).
+template <typename T>
+void lasso_mask(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha,
+                const Matrix<bool>& mask, int L, const T constraint, const T lambda2 = 0,
+                constraint_type mode = PENALTY, const bool pos = false,
+                const int numThreads = -1) {
+  (void)numThreads;
+  namespace d = spams_b200_detail;
+  typename d::Csc<T>::type out;
+  d::check(d::call_lasso_mask(X.X(), (int)X.m(), X.n(), D.X(), (int)D.n(), mask.X(), L,
+                              constraint, lambda2, (int)mode, pos ? 1 : 0, &out));
+  d::adopt<T>(out, spalpha);
 }
 
 #endif  // SPAMS_B200_DECOMP_H

@@ -1,7 +1,7 @@
 // Drives the drop-in C++ API (include/spams_b200/cppspams.h) the way the
 // reference's own demo drives cppspams.h (cpp_library/test_decomp.cpp:14-64):
 // OMP and LARS-Lasso on a dictionary and a batch of signals, through
-// cppOMP / cppLasso / _omp / _lassoD / lasso2(G, DtX).  Inputs and outputs are
+// cppOMP / cppLasso / _omp / _lassoD / lasso2(G, DtX) / _ompMask / _lassoMask.  Inputs and outputs are
 // raw binary files in a directory given on the command line; the GPU test
 // suite compares the outputs with the oracle.
 #include <cstdio>
@@ -97,6 +97,27 @@ static int run(const std::string& dir, int m, int n, int K) {
     SpMatrix<T>* sp2 = cppLasso(X, G, DtX, &path, false, -1, T(0.15));
     write_csc(dir + "/lasso_qq.csc", *sp2);
     delete sp2;
+  }
+  // masked variants: row r of signal i observed unless (7 r + 3 i) % 10 >= 7;
+  // signal 0 fully observed, signal 1 not at all
+  {
+    std::vector<char> bm((size_t)m * n);
+    for (int i = 0; i < n; ++i)
+      for (int r = 0; r < m; ++r)
+        bm[(size_t)i * m + r] = i == 0 ? 1 : (i == 1 ? 0 : ((7 * r + 3 * i) % 10 < 7));
+    Matrix<bool> B(reinterpret_cast<bool*>(bm.data()), m, n);
+    Vector<int> Lv(1);
+    Lv[0] = 6;
+    Vector<T> eps(1), la(1);
+    eps[0] = 0;
+    la[0] = 0;
+    Matrix<T>* path = nullptr;
+    SpMatrix<T>* spa = _ompMask(&X, &D, &B, &path, false, true, &Lv, true, &eps, true, &la, -1);
+    write_csc(dir + "/omp_mask.csc", *spa);
+    delete spa;
+    SpMatrix<T>* spl = _lassoMask(&X, &D, &B, -1, T(0.1), T(0), PENALTY, false, -1, false);
+    write_csc(dir + "/lasso_mask.csc", *spl);
+    delete spl;
   }
   // facade error path
   {

@@ -51,6 +51,14 @@ def test_cpp_dropin(tmp_path, std, prec):
         "lasso_gram": O.orc_lasso(X64, D64, lambda1=0.15),
         "lasso_qq": O.orc_lasso(X64, D64, lambda1=0.15),
     }
+    rr, ii = np.meshgrid(np.arange(48), np.arange(400), indexing="ij")
+    B = (7 * rr + 3 * ii) % 10 < 7
+    B[:, 0] = True
+    B[:, 1] = False
+    cases["omp_mask"] = O.orc_omp_mask(X64, D64, B, L=6, eps=0.0, lambda1=0.0)
+    lm = O.orc_lasso_mask(X64, D64, B, lambda1=0.1).copy()
+    lm.eliminate_zeros()
+    cases["lasso_mask"] = lm
     for name, ref in cases.items():
         a = _read_csc(tmp_path / f"{name}.csc")
         assert a.shape == ref.shape, name
