@@ -83,7 +83,11 @@ typedef struct {
   int kernel;     /* SC_KERNEL_*: which coding kernels may run; default
                      SC_KERNEL_AUTO (timed once per shape, then cached).
                      Every choice gives the same results. */
-  int reserved[3];
+  int refactor;   /* single-precision Lasso: 0 (default) rebuilds the active
+                     set's inverse Gram in FP64 when an added atom's pivot
+                     falls below 1e-3 of its diagonal (active sets up to 32
+                     atoms); > 0 on every added atom; < 0 never */
+  int reserved[2];
 } sc_options;
 
 /* Coding kernels: one warp per signal (up to 1024 atoms) or one CTA of

@@ -21,6 +21,7 @@
 #include "../../include/spams_b200.h"
 #include "engine.h"
 #include "kernels.h"
+#include "refactor.cuh"
 
 namespace sc {
 
@@ -357,6 +358,7 @@ struct Problem {
   bool refine = false;            // FP64 refinement of the final coefficients
   bool ols = false;               // least-squares refit on the final support (lasso ols)
   int kernel = SC_KERNEL_AUTO;    // SC_KERNEL_*: kernel family (AUTO: tuned)
+  int refactor = 1;               // LARS FP64 refactor: 0 never, 1 small pivots, 2 always
   // masked variants (lasso_mask / omp_mask): host row mask m x n, the ridge of
   // the masked Grams, and whether the Lasso constraint is scaled by the
   // observed fraction (PENALTY / L2ERROR; OMP always scales eps)
@@ -400,16 +402,26 @@ struct HostSink {
 };
 
 // Host-array calls code their signals in chunks of about n / kPipeChunks
-// (at least kPipeMinChunk signals): while one chunk is coded, the next one is
-// copied in on the H2D stream and the previous chunk's CSC is read back.
-constexpr int kPipeChunks = 6;
+// (at least kPipeMinChunk signals) after a first chunk a quarter of that size:
+// while one chunk is coded, the next one is copied in on the H2D stream and
+// the previous chunk's CSC is read back.  (Measured on the 100k-signal lasso
+// workload: 3.74 ms end to end against 3.84 with six equal chunks; a second
+// coding stream for alternate chunks was slower, 4.29 ms.)
+constexpr int kPipeChunks = 5;
 constexpr int64_t kPipeMinChunk = 16384;
+constexpr int64_t kPipeFirstDiv = 4;
 
 template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
-  const std::vector<Shape> cands = shape_candidates<T>(c, p.lars, Kp, p.L, p.kernel);
+  std::vector<Shape> cands = shape_candidates<T>(c, p.lars, Kp, p.L, p.kernel);
+  // FP64 refactor of single-precision LARS: one 16 KB scratch per warp (warp
+  // kernels) or CTA (CTA kernels, whose grid is then fixed here)
+  const bool refac = p.lars && sizeof(T) == 4 && p.refactor != 0;
+  if (refac)
+    for (Shape& sh : cands)
+      if (sh.cta) sh.grid = lars_cta_grid<T>(Kp, sh.Lcap, false);
   const bool piped = sink && p.hX && !p.hmask;
   const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
@@ -467,6 +479,16 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   };
   for (const Shape& sh : cands)
     if (sh.Lcap < p.L) SC_TRY(c.gstate.reserve(ovf_plan(sh).bytes));
+  const size_t rf_unit = (size_t)2 * kRefactorMax * kRefactorMax * sizeof(double);
+  if (refac) {
+    size_t units = 0;
+    for (const Shape& sh : cands) {
+      units = std::max(units, (size_t)sh.grid * (sh.cta ? 1 : sh.wpb));
+      const Ovf ov = ovf_plan(sh);
+      units = std::max(units, (size_t)ov.grid * ov.wpb);
+    }
+    SC_TRY(c.rfscr.reserve(units * rf_unit));
+  }
   // masked variants: Dᵀ, the chunk's mask / classes / scaled parameters, and
   // one m-vector of scratch per warp of the largest launch
   MaskArgs<T> mk{};
@@ -500,8 +522,16 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
   g_prof.signals += p.n;
 
-  const int64_t nchunks = p.n > 0 ? (p.n + nc - 1) / nc : 0;
-  auto chunk_len = [&](int64_t i) { return std::min<int64_t>(nc, p.n - i * nc); };
+  // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i)).
+  // With the pipeline the first chunk is 1/kPipeFirstDiv of the others: its
+  // copy-in is the only one nothing overlaps.
+  const int64_t first = piped ? std::max<int64_t>(1, std::min<int64_t>(p.n, nc / kPipeFirstDiv)) : nc;
+  const int64_t nchunks =
+      p.n <= 0 ? 0 : (p.n <= first ? 1 : 1 + (p.n - first + nc - 1) / nc);
+  auto chunk_start = [&](int64_t i) { return i == 0 ? (int64_t)0 : first + (i - 1) * nc; };
+  auto chunk_len = [&](int64_t i) {
+    return std::min<int64_t>(i == 0 ? first : nc, p.n - chunk_start(i));
+  };
   auto xslot_ptr = [&](int64_t i) {
     return reinterpret_cast<T*>(static_cast<char*>(c.xstage.ptr) + (i & 1) * (piped ? xslot : 0));
   };
@@ -510,7 +540,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   auto issue_h2d = [&](int64_t i) -> sc_status {
     cudaStream_t cs = piped ? c.h2d_stream : st;
     if (piped) SC_CUDA(cudaStreamWaitEvent(cs, c.ev_xfree[i & 1], 0));
-    SC_CUDA(cudaMemcpyAsync(xslot_ptr(i), p.hX + (size_t)(i * nc) * p.m,
+    SC_CUDA(cudaMemcpyAsync(xslot_ptr(i), p.hX + (size_t)chunk_start(i) * p.m,
                             (size_t)chunk_len(i) * p.m * sizeof(T), cudaMemcpyHostToDevice, cs));
     if (piped) SC_CUDA(cudaEventRecord(c.ev_h2d[i & 1], cs));
     return SC_OK;
@@ -537,7 +567,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       SC_CUDA(cudaEventRecord(c.ev_d2h[slot], cs));
       SC_CUDA(cudaEventSynchronize(c.ev_d2h[slot]));
     }
-    int64_t* dst = sink->colptr + i * nc;
+    int64_t* dst = sink->colptr + chunk_start(i);
     for (int64_t k = 0; k <= cn; ++k) dst[k] = nnz_total + hcol[k];
     nnz_total += cnnz;
     sink->nnz = (size_t)nnz_total;
@@ -599,7 +629,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_TRY(issue_h2d(0));
   }
   for (int64_t ci = 0; ci < nchunks; ++ci) {
-    const int64_t start = ci * nc;
+    const int64_t start = chunk_start(ci);
     const int64_t cn = chunk_len(ci);
     T* dtx = reinterpret_cast<T*>(c.dtx.ptr);
     T* norms = reinterpret_cast<T*>(c.norms.ptr);
@@ -676,6 +706,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.gstate = nullptr; a.path = final_run ? path : nullptr;
         a.steps = final_run ? d_steps : nullptr;
         a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
+        a.refactor = refac ? p.refactor : 0;
+        a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
         if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
         else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
         if (final_run) pr.launches(1);
@@ -991,6 +1023,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
   if (mask) {  // omp_mask: masked Grams get a 1e-10 ridge, eps scales (decomp/decomp.h:477-481)
     p.hmask = mask;
     p.mask_ridge = T(1e-10);
@@ -1100,6 +1133,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
   if (mask) {
     // lasso_mask: ridge max(lambda2, 1e-10) on the masked Grams, PENALTY and
     // L2ERROR constraints scaled by the observed fraction, coreLARS2's default
@@ -1178,6 +1212,7 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);
@@ -1222,6 +1257,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
+  p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, nullptr, d_capflag, pr));
   if (nnz_out) SC_TRY(check_tc<T>(*c, st, p));
   return finish_dev<T>(c, st, d_colptr, n, d_capflag, nnz_out);

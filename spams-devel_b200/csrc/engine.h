@@ -60,10 +60,12 @@ struct DeviceCtx {
   Buf X, D, G, dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, gstate;
   Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
   Buf mask, mflag, mvec, Dt, mwork;  // masked variants
+  Buf rfscr;                         // FP64 refactor scratch of the LARS kernels
   std::vector<Buf*> all_bufs() {
     return {&X, &D, &G, &dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc,
             &scan, &gstate, &ccolptr, &crows, &cvals, &path, &vecs, &xstage, &xsplit,
-            &dsplit, &level, &rlist, &rscratch, &mask, &mflag, &mvec, &Dt, &mwork};
+            &dsplit, &level, &rlist, &rscratch, &mask, &mflag, &mvec, &Dt, &mwork,
+            &rfscr};
   }
 };
 

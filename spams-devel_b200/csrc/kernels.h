@@ -70,6 +70,12 @@ struct LarsArgs {
   unsigned long long* steps;  // if set: total homotopy steps are added here
   T* out_level;        // if set: n correlation levels of the final active sets
   MaskArgs<T> mk;      // masked variant (mk.mask set), warp kernels only
+  // FP64 refactor of the single-precision inverse Gram (refactor.cuh):
+  // 0 never, 1 when an added atom's relative pivot falls below
+  // kRefactorPivot, 2 on every added atom; rf_scratch: 2 x 32 x 32 doubles per
+  // warp (warp kernels) or per CTA (CTA kernels) of the launch
+  int refactor;
+  double* rf_scratch;
 };
 
 template <typename T>
@@ -114,6 +120,9 @@ template <typename T>
 size_t lars_cta_smem_bytes(int Kp, int Lc, bool gstate);
 template <typename T>
 size_t lars_cta_gstate_bytes(int Lc, int grid);
+// The persistent grid the CTA launcher fills the device with (0 on error).
+template <typename T>
+int lars_cta_grid(int Kp, int Lc, bool gstate);
 
 template <typename T>
 cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);

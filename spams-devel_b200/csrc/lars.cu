@@ -21,6 +21,7 @@
 // a global scratch slab per warp.
 #include "common.cuh"
 #include "kernels.h"
+#include "refactor.cuh"
 #include "masked.cuh"
 
 namespace sc {
@@ -173,8 +174,17 @@ lars_kernel(const LarsArgs<T> a) {
             T part = 0;
             for (int r = lane; r < i; r += 32) part += sW[r] * sG[r];
             const T dot = warp_sum(part);
-            const T schur = T(1) / (sG[i] - dot);
-            for (int r = lane; r < i; r += 32) {
+            const T piv = sG[i] - dot;
+            // a small pivot loses digits in the update: rebuild the inverse in FP64
+            bool refactored = false;
+            if (sizeof(T) == 4 && a.refactor && i < kRefactorMax && !partial &&
+                (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
+              double* rs = a.rf_scratch + (size_t)(blockIdx.x * wpb + wib) * (2 * kRefactorMax * kRefactorMax);
+              refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs,
+                                               rs + kRefactorMax * kRefactorMax);
+            }
+            const T schur = T(1) / piv;
+            if (!refactored) for (int r = lane; r < i; r += 32) {
               T* row = sInv + (size_t)r * ldi;
               const T wr = sW[r];
               for (int c = 0; c < i; ++c) {
@@ -186,7 +196,7 @@ lars_kernel(const LarsArgs<T> a) {
               row[i] = off;
               sInv[(size_t)i * ldi + r] = off;
             }
-            if (lane == 0) sInv[(size_t)i * ldi + i] = schur;
+            if (lane == 0 && !refactored) sInv[(size_t)i * ldi + i] = schur;
           }
           __syncwarp();
         }

@@ -11,6 +11,7 @@
 // Used for Kp = 512 .. 4096 (W = Kp / 512) and active-set capacities up to L.
 #include "common.cuh"
 #include "kernels.h"
+#include "refactor.cuh"
 
 namespace sc {
 
@@ -179,8 +180,17 @@ lars_cta_kernel(const LarsArgs<T> a) {
               T part = 0;
               for (int r = lane; r < i; r += 32) part += sW[r] * sG[r];
               const T dot = warp_sum(part);
-              const T schur = T(1) / (sG[i] - dot);
-              for (int r = lane; r < i; r += 32) {
+              const T piv = sG[i] - dot;
+              // a small pivot loses digits in the update: rebuild the inverse in FP64
+              bool refactored = false;
+              if (sizeof(T) == 4 && a.refactor && i < kRefactorMax && !false &&
+                  (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
+                double* rs = a.rf_scratch + (size_t)blockIdx.x * (2 * kRefactorMax * kRefactorMax);
+                refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs,
+                                                 rs + kRefactorMax * kRefactorMax);
+              }
+              const T schur = T(1) / piv;
+              if (!refactored) for (int r = lane; r < i; r += 32) {
                 T* row = sInv + (size_t)r * ldi;
                 const T wr = sW[r];
                 for (int c = 0; c < i; ++c) {
@@ -192,7 +202,7 @@ lars_cta_kernel(const LarsArgs<T> a) {
                 row[i] = off;
                 sInv[(size_t)i * ldi + r] = off;
               }
-              if (lane == 0) sInv[(size_t)i * ldi + i] = schur;
+              if (lane == 0 && !refactored) sInv[(size_t)i * ldi + i] = schur;
             }
             __syncwarp();
           }
@@ -441,6 +451,31 @@ size_t lars_cta_gstate_bytes(int Lc, int grid) {
   return (size_t)grid * lars_cta_state(Lc, sizeof(T));
 }
 
+template <typename T, int W>
+static int grid_w(size_t smem) {
+  auto k = lars_cta_kernel<T, W>;
+  int grid = 0;
+  if (allow_smem(k, smem) != cudaSuccess || fill_grid(k, W * 32, smem, &grid) != cudaSuccess)
+    return 0;
+  return grid;
+}
+
+template <typename T>
+int lars_cta_grid(int Kp, int Lc, bool gstate) {
+  const size_t smem = lars_cta_smem_bytes<T>(Kp, Lc, gstate);
+  switch (Kp / 512) {
+    case 1: return grid_w<T, 1>(smem);
+    case 2: return grid_w<T, 2>(smem);
+    case 3: return grid_w<T, 3>(smem);
+    case 4: return grid_w<T, 4>(smem);
+    case 5: return grid_w<T, 5>(smem);
+    case 6: return grid_w<T, 6>(smem);
+    case 7: return grid_w<T, 7>(smem);
+    case 8: return grid_w<T, 8>(smem);
+    default: return 0;
+  }
+}
+
 template <typename T>
 cudaError_t launch_lars_cta(const LarsArgs<T>& a, int grid, cudaStream_t st) {
   if (a.Kp % 512 != 0) return cudaErrorInvalidValue;
@@ -462,6 +497,8 @@ template size_t lars_cta_smem_bytes<float>(int, int, bool);
 template size_t lars_cta_smem_bytes<double>(int, int, bool);
 template size_t lars_cta_gstate_bytes<float>(int, int);
 template size_t lars_cta_gstate_bytes<double>(int, int);
+template int lars_cta_grid<float>(int, int, bool);
+template int lars_cta_grid<double>(int, int, bool);
 template cudaError_t launch_lars_cta<float>(const LarsArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_lars_cta<double>(const LarsArgs<double>&, int, cudaStream_t);
 

@@ -58,7 +58,8 @@ class CscF64(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("profile", C.c_int),
-                ("refine", C.c_int), ("kernel", C.c_int), ("reserved", C.c_int * 3)]
+                ("refine", C.c_int), ("kernel", C.c_int), ("refactor", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class Profile(C.Structure):

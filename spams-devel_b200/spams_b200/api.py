@@ -40,8 +40,12 @@ _KERNELS = {None: 0, "auto": 0, "warp": 1, "cta": 2}
 
 
 def _opts(precision: Optional[int], device: int, profile: bool = False,
-          refine: Optional[bool] = None, kernel: Optional[str] = None) -> Options:
+          refine: Optional[bool] = None, kernel: Optional[str] = None,
+          refactor: Optional[str] = None) -> Options:
     o = Options()
+    if refactor not in (None, "pivot", "always", "never"):
+        raise ValueError("spams_b200: refactor must be 'pivot', 'always' or 'never'")
+    o.refactor = {None: 0, "pivot": 0, "always": 1, "never": -1}[refactor]
     o.precision = SC_PREC_FP32 if precision is None else int(precision)
     o.device = int(device)
     o.profile = int(bool(profile))
@@ -151,7 +155,7 @@ def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=
 def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, lambda2=0.,
           mode=SC_PENALTY, pos=False, ols=False, numThreads=-1, max_length_path=-1,
           verbose=False, cholesky=False, precision=None, device=0, refine=None,
-          kernel=None):
+          kernel=None, refactor=None):
     """LARS-Lasso of every column of X (swig/python/spams.py:109-142).
 
     mode 0: ||a||_1 <= lambda1; 1: ||x - D a||^2 <= lambda1; 2 (default):
@@ -170,7 +174,7 @@ def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, 
     f64 = dt == np.float64
     ct = C.c_double if f64 else C.c_float
     out = CscF64() if f64 else CscF32()
-    o = _opts(precision, device, refine=refine, kernel=kernel)
+    o = _opts(precision, device, refine=refine, kernel=kernel, refactor=refactor)
     if Q is not None:
         Q = _fortran(Q, dt)
         q = _fortran(q, dt)

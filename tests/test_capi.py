@@ -124,3 +124,10 @@ def test_mask_front_ends_check_arguments_without_a_device():
         spams_b200.lassoMask(X, D, B)
     with pytest.raises(ValueError, match="incompatible matrix dimensions"):
         spams_b200.lassoMask(X, np.asfortranarray(np.random.randn(9, 6)), B, lambda1=0.1)
+
+
+def test_refactor_choice_is_validated():
+    X = np.asfortranarray(np.random.randn(8, 4).astype(np.float32))
+    D = np.asfortranarray(np.random.randn(8, 6).astype(np.float32))
+    with pytest.raises(ValueError, match="refactor must be"):
+        spams_b200.lasso(X, D, lambda1=0.1, refactor="sometimes")
