@@ -18,7 +18,7 @@ constexpr double kRefactorPivot = 1e-3;  // relative pivot that triggers it
 // global scratch.  Returns false and writes nothing when G_AA is not
 // positive definite in double.
 template <typename T>
-__device__ bool refactor_inverse(const T* __restrict__ G, int Kp, const int* ind, int n, T* inv,
+__device__ __noinline__ bool refactor_inverse(const T* __restrict__ G, int Kp, const int* ind, int n, T* inv,
                                  int ldi, double* A, double* B) {
   const int lane = threadIdx.x & 31;
   constexpr int ld = kRefactorMax;
