@@ -320,15 +320,18 @@ def run_ours(args) -> None:
     h2d = Xf.nbytes + Df.nbytes
     d2h = (n + 1) * 8 + a.nnz * 8
 
-    # ---- CPU baseline (rank 0, one GPU only)
+    # ---- CPU baseline (rank 0, one GPU only): all host threads, and one
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, sample = cpu_reference_rate(Xf, Df, args.cpu_seconds, -1)
+            rate1, sample1 = cpu_reference_rate(Xf, Df, max(1.0, args.cpu_seconds / 3), 1)
             thr = omp_threads(-1)
             cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "reference",
                    "sample": f"first {sample} signals of the workload, reference lasso2 "
-                             f"(T=float), OpenMP {thr} threads, OPENBLAS_NUM_THREADS=1"}
+                             f"(T=float), OpenMP {thr} threads, OPENBLAS_NUM_THREADS=1",
+                   "single_thread_value": rate1,
+                   "single_thread_sample": f"first {sample1} signals, numThreads=1"}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
