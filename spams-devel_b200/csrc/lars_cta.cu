@@ -48,7 +48,9 @@ __host__ __device__ inline size_t lars_cta_smem(int Kp, int Lc, size_t esz, int 
          (gstate ? 0 : lars_cta_state(Lc, esz));
 }
 
-template <typename T, int W>
+// MODE >= 0 fixes the constraint mode at compile time (PENALTY without pos
+// prunes the other modes' code); -1 reads it from a.
+template <typename T, int W, int MODE = -1>
 __global__ void __launch_bounds__(W * 32)
 lars_cta_kernel(const LarsArgs<T> a) {
   constexpr int NV = 4;  // 128-row chunks per warp
@@ -80,8 +82,8 @@ lars_cta_kernel(const LarsArgs<T> a) {
   const T INF = inf<T>();
   const int L = a.L < K ? a.L : K;
   const int length_path = a.length_path <= 1 ? 4 * L : a.length_path;
-  const int mode = a.mode;
-  const bool pos = a.pos != 0;
+  const int mode = MODE >= 0 ? MODE : a.mode;
+  const bool pos = MODE >= 0 ? false : a.pos != 0;
   const int n_jobs = a.n_jobs_dev ? *a.n_jobs_dev : a.n_jobs;
   const int rbase = gw * NV * 128;
 
@@ -433,7 +435,7 @@ lars_cta_kernel(const LarsArgs<T> a) {
 
 template <typename T, int W>
 static cudaError_t launch_w(const LarsArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-  auto k = lars_cta_kernel<T, W>;
+  auto k = (a.mode == 2 && !a.pos) ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
@@ -452,8 +454,8 @@ size_t lars_cta_gstate_bytes(int Lc, int grid) {
 }
 
 template <typename T, int W>
-static int grid_w(size_t smem) {
-  auto k = lars_cta_kernel<T, W>;
+static int grid_w(size_t smem, bool penalty) {
+  auto k = penalty ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
   int grid = 0;
   if (allow_smem(k, smem) != cudaSuccess || fill_grid(k, W * 32, smem, &grid) != cudaSuccess)
     return 0;
@@ -461,17 +463,17 @@ static int grid_w(size_t smem) {
 }
 
 template <typename T>
-int lars_cta_grid(int Kp, int Lc, bool gstate) {
+int lars_cta_grid(int Kp, int Lc, bool gstate, bool penalty) {
   const size_t smem = lars_cta_smem_bytes<T>(Kp, Lc, gstate);
   switch (Kp / 512) {
-    case 1: return grid_w<T, 1>(smem);
-    case 2: return grid_w<T, 2>(smem);
-    case 3: return grid_w<T, 3>(smem);
-    case 4: return grid_w<T, 4>(smem);
-    case 5: return grid_w<T, 5>(smem);
-    case 6: return grid_w<T, 6>(smem);
-    case 7: return grid_w<T, 7>(smem);
-    case 8: return grid_w<T, 8>(smem);
+    case 1: return grid_w<T, 1>(smem, penalty);
+    case 2: return grid_w<T, 2>(smem, penalty);
+    case 3: return grid_w<T, 3>(smem, penalty);
+    case 4: return grid_w<T, 4>(smem, penalty);
+    case 5: return grid_w<T, 5>(smem, penalty);
+    case 6: return grid_w<T, 6>(smem, penalty);
+    case 7: return grid_w<T, 7>(smem, penalty);
+    case 8: return grid_w<T, 8>(smem, penalty);
     default: return 0;
   }
 }
@@ -497,8 +499,8 @@ template size_t lars_cta_smem_bytes<float>(int, int, bool);
 template size_t lars_cta_smem_bytes<double>(int, int, bool);
 template size_t lars_cta_gstate_bytes<float>(int, int);
 template size_t lars_cta_gstate_bytes<double>(int, int);
-template int lars_cta_grid<float>(int, int, bool);
-template int lars_cta_grid<double>(int, int, bool);
+template int lars_cta_grid<float>(int, int, bool, bool);
+template int lars_cta_grid<double>(int, int, bool, bool);
 template cudaError_t launch_lars_cta<float>(const LarsArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_lars_cta<double>(const LarsArgs<double>&, int, cudaStream_t);
 
