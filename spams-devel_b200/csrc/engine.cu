@@ -324,6 +324,10 @@ struct TuneKey {
 static std::mutex g_tune_mu;
 static std::map<TuneKey, int> g_tune;  // key -> index into shape_candidates
 
+// A candidate replaces the one kept so far only below this fraction of its
+// sample time.
+constexpr float kTuneMargin = 0.95f;
+
 static bool autotune_enabled() {
   static const bool on = [] {
     const char* e = getenv("SC_AUTOTUNE");
@@ -613,7 +617,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       cudaEventSynchronize(e1);
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (i == 0 || ms < best_ms) { best = (int)i; best_ms = ms; }
+      // the static rule's shape (candidate 0) is kept unless another one is
+      // clearly faster on the sample: near-ties decided by timing noise made
+      // the choice, and so the full-batch speed, vary from run to run
+      if (i == 0 || ms < best_ms * kTuneMargin) { best = (int)i; best_ms = ms; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
