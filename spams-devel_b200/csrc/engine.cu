@@ -391,6 +391,18 @@ struct HostSink {
     if (!colptr) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
     return SC_OK;
   }
+  // Best-effort capacity for `want` entries (a failed allocation is left to
+  // grow()).
+  void hint(size_t want) {
+    if (want <= cap) return;
+    int32_t* r = (int32_t*)realloc(rows, want * sizeof(int32_t));
+    if (!r) return;
+    rows = r;
+    T* v = (T*)realloc(vals, want * sizeof(T));
+    if (!v) return;  // rows keeps its larger block; cap still describes vals
+    vals = v;
+    cap = want;
+  }
   sc_status grow(size_t need) {
     if (need <= cap) return SC_OK;
     size_t c2 = std::max(need, cap + cap / 2);
@@ -406,14 +418,17 @@ struct HostSink {
 };
 
 // Host-array calls code their signals in chunks of about n / kPipeChunks
-// (at least kPipeMinChunk signals) after a first chunk a quarter of that size:
-// while one chunk is coded, the next one is copied in on the H2D stream and
-// the previous chunk's CSC is read back.  (Measured on the 100k-signal lasso
-// workload: 3.74 ms end to end against 3.84 with six equal chunks; a second
-// coding stream for alternate chunks was slower, 4.29 ms.)
+// (at least kPipeMinChunk signals) after a first chunk half that size: while
+// one chunk is coded, the next one is copied in on the H2D stream and the
+// previous chunk's CSC is read back.  The result arrays are sized after the
+// first chunk from its entries per signal (one allocation instead of a
+// growing series of reallocations and copies).  Measured on the 100k-signal
+// lasso workload: 3.31 ms end to end against 3.36 with a quarter-size first
+// chunk and growth by reallocation, 3.30-3.94 ms for 3 to 8 chunks; a second
+// coding stream for alternate chunks was slower.
 constexpr int kPipeChunks = 5;
 constexpr int64_t kPipeMinChunk = 16384;
-constexpr int64_t kPipeFirstDiv = 4;
+constexpr int64_t kPipeFirstDiv = 2;
 
 template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
@@ -559,6 +574,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     const int64_t* hcol =
         reinterpret_cast<const int64_t*>(static_cast<char*>(c.pinned_col) + slot * col_slot);
     const int64_t cnnz = hcol[cn];
+    if (i == 0 && p.n > cn)  // the whole result at the first chunk's density, +15%
+      sink->hint((size_t)((double)cnnz * (double)p.n / (double)cn * 1.15) + 1024);
     SC_TRY(sink->grow((size_t)(nnz_total + cnnz)));
     if (cnnz > 0) {
       cudaStream_t cs = piped ? c.d2h_stream : st;
