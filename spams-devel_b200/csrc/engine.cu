@@ -246,7 +246,7 @@ constexpr int kCtaMaxKp = 4096;
 // kernel holds larger active sets in shared memory and codes each signal
 // with more threads (lower latency when the batch is small or the active
 // sets outgrow the warp's capacity and take the overflow rerun).  The first
-// call of each (algorithm, precision, Kp, L, batch-size class) times every
+// call of each (algorithm, precision, Kp, L class, batch-size class) times every
 // candidate on its first chunk and keeps the fastest; SC_AUTOTUNE=0 in the
 // environment selects the static rule instead (warp up to 1024 atoms).
 struct Shape {
@@ -275,7 +275,7 @@ static Shape warp_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap) {
 }
 
 template <typename T>
-static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
+static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap = 80) {
   Shape s;
   s.cta = true;
   s.wpb = Kp / 512;
@@ -285,7 +285,7 @@ static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
   auto bytes = [&](int lc) {
     return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
   };
-  s.Lcap = std::max(1, std::min(L, 80));
+  s.Lcap = std::max(1, std::min(L, cap));
   while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
                          2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
     s.Lcap -= 16;
@@ -309,16 +309,21 @@ static std::vector<Shape> shape_candidates(const DeviceCtx& c, bool lars, int Kp
     v.push_back(warp_shape<T>(c, lars, Kp, L, 32));
     if (L > 32) v.push_back(warp_shape<T>(c, lars, Kp, L, 64));
   }
-  if (cta_ok && kernel != SC_KERNEL_WARP) v.push_back(cta_shape<T>(c, lars, Kp, L));
+  if (cta_ok && kernel != SC_KERNEL_WARP) {
+    v.push_back(cta_shape<T>(c, lars, Kp, L));
+    // a 32-atom state leaves room for more CTAs per SM; larger active sets
+    // take the overflow rerun
+    if (L > 32) v.push_back(cta_shape<T>(c, lars, Kp, L, 32));
+  }
   if (v.empty()) v.push_back(pick_shape<T>(c, lars, Kp, L));
   return v;
 }
 
 struct TuneKey {
-  int lars, dbl, Kp, L, nclass, kernel;
+  int lars, dbl, Kp, lclass, nclass, kernel;
   bool operator<(const TuneKey& o) const {
-    return std::tie(lars, dbl, Kp, L, nclass, kernel) <
-           std::tie(o.lars, o.dbl, o.Kp, o.L, o.nclass, o.kernel);
+    return std::tie(lars, dbl, Kp, lclass, nclass, kernel) <
+           std::tie(o.lars, o.dbl, o.Kp, o.lclass, o.nclass, o.kernel);
   }
 };
 static std::mutex g_tune_mu;
@@ -598,7 +603,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // kernel family: a single candidate, the cached choice of an earlier call,
   // the static rule, or timed on the first chunk (tune)
   int chosen = cands.size() == 1 ? 0 : -1;
-  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, p.L, 0, p.kernel};
+  // L enters by class only (the candidate shapes differ at 32 and 64 atoms):
+  // a serving stream's batches carry many different L
+  const int lclass = p.L <= 32 ? 0 : (p.L <= 64 ? 1 : 2);
+  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, lclass, 0, p.kernel};
   {
     int64_t c0 = std::min<int64_t>(nc, p.n), cls = 0;
     while (c0 > 1) { c0 >>= 1; ++cls; }
@@ -621,27 +629,33 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     cudaEvent_t e0, e1;
     SC_CUDA(cudaEventCreate(&e0));
     SC_CUDA(cudaEventCreate(&e1));
-    int best = 0;
-    float best_ms = 0;
+    // two interleaved rounds, the faster time of each candidate
+    std::vector<float> t(cands.size(), 0.f);
     sc_status stt = SC_OK;
-    for (size_t i = 0; i < cands.size() && stt == SC_OK; ++i) {
-      stt = code(cands[i], std::min<int64_t>(sample, 64), false);  // module load, attributes
-      if (stt != SC_OK) break;
-      cudaEventRecord(e0, st);
-      stt = code(cands[i], sample, false);
-      cudaEventRecord(e1, st);
-      if (stt != SC_OK) break;
-      cudaEventSynchronize(e1);
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      // the static rule's shape (candidate 0) is kept unless another one is
-      // clearly faster on the sample: near-ties decided by timing noise made
-      // the choice, and so the full-batch speed, vary from run to run
-      if (i == 0 || ms < best_ms * kTuneMargin) { best = (int)i; best_ms = ms; }
-    }
+    for (int round = 0; round < 2 && stt == SC_OK; ++round)
+      for (size_t i = 0; i < cands.size() && stt == SC_OK; ++i) {
+        if (round == 0) {
+          stt = code(cands[i], std::min<int64_t>(sample, 64), false);  // module load, attributes
+          if (stt != SC_OK) break;
+        }
+        cudaEventRecord(e0, st);
+        stt = code(cands[i], sample, false);
+        cudaEventRecord(e1, st);
+        if (stt != SC_OK) break;
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (round == 0 || ms < t[i]) t[i] = ms;
+      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (stt != SC_OK) return stt;
+    // the static rule's shape (candidate 0) is kept unless another one is
+    // clearly faster on the sample: near-ties decided by timing noise made
+    // the choice, and so the full-batch speed, vary from run to run
+    int best = 0;
+    for (size_t i = 1; i < cands.size(); ++i)
+      if (t[i] < t[(size_t)best] * kTuneMargin) best = (int)i;
     out = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
