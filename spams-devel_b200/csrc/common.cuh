@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #define SC_INF_F (__int_as_float(0x7f800000))
 
@@ -213,6 +216,33 @@ inline cudaError_t allow_smem(Kern k, size_t smem) {
   e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
+// Of two builds of one kernel, the second compiled with a register bound,
+// the one that keeps more CTAs resident per SM with `smem` bytes of dynamic
+// shared memory; the unbounded build on ties (the bound only costs spills
+// when shared memory or threads limit residency anyway).
+// The answer is kept per (kernel, threads, shared memory, device).
+template <typename Kern>
+inline Kern more_resident(Kern plain, Kern bounded, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t, int>, bool> memo;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return plain;
+  const auto key = std::make_tuple((const void*)plain, threads, smem, dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second ? bounded : plain;
+  }
+  int a = 0, b = 0;
+  if (allow_smem(plain, smem) != cudaSuccess || allow_smem(bounded, smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, plain, threads, smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bounded, threads, smem) != cudaSuccess)
+    return plain;
+  std::lock_guard<std::mutex> lk(mu);
+  memo[key] = b > a;
+  return b > a ? bounded : plain;
 }
 
 }  // namespace sc

@@ -275,7 +275,7 @@ static Shape warp_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap) {
 }
 
 template <typename T>
-static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap = 80) {
+static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
   Shape s;
   s.cta = true;
   s.wpb = Kp / 512;
@@ -285,7 +285,7 @@ static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap = 8
   auto bytes = [&](int lc) {
     return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
   };
-  s.Lcap = std::max(1, std::min(L, cap));
+  s.Lcap = std::max(1, std::min(L, 80));
   while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
                          2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
     s.Lcap -= 16;
@@ -309,12 +309,7 @@ static std::vector<Shape> shape_candidates(const DeviceCtx& c, bool lars, int Kp
     v.push_back(warp_shape<T>(c, lars, Kp, L, 32));
     if (L > 32) v.push_back(warp_shape<T>(c, lars, Kp, L, 64));
   }
-  if (cta_ok && kernel != SC_KERNEL_WARP) {
-    v.push_back(cta_shape<T>(c, lars, Kp, L));
-    // a 32-atom state leaves room for more CTAs per SM; larger active sets
-    // take the overflow rerun
-    if (L > 32) v.push_back(cta_shape<T>(c, lars, Kp, L, 32));
-  }
+  if (cta_ok && kernel != SC_KERNEL_WARP) v.push_back(cta_shape<T>(c, lars, Kp, L));
   if (v.empty()) v.push_back(pick_shape<T>(c, lars, Kp, L));
   return v;
 }

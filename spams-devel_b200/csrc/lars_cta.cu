@@ -50,12 +50,8 @@ __host__ __device__ inline size_t lars_cta_smem(int Kp, int Lc, size_t esz, int 
 
 // MODE >= 0 fixes the constraint mode at compile time (PENALTY without pos
 // prunes the other modes' code); -1 reads it from a.
-// Single precision with W >= 4 warps: at most 64 registers (four CTAs per SM
-// on 2048-4096 atoms; 2.57 -> 2.34 ms per 20k signals on 4096 atoms); with
-// fewer warps the bound spilled and ran slower.
-template <typename T, int W, int MODE = -1>
-__global__ void __launch_bounds__(W * 32, (sizeof(T) == 4 && W >= 4) ? 32 / W : 1)
-lars_cta_kernel(const LarsArgs<T> a) {
+template <typename T, int W, int MODE>
+__device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   constexpr int NV = 4;  // 128-row chunks per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -436,9 +432,33 @@ lars_cta_kernel(const LarsArgs<T> a) {
   }
 }
 
+template <typename T, int W, int MODE = -1>
+__global__ void __launch_bounds__(W * 32) lars_cta_kernel(const LarsArgs<T> a) {
+  lars_cta_body<T, W, MODE>(a);
+}
+// The same kernel built with at most 64 registers, taken only where it keeps
+// more CTAs resident (2.57 -> 2.34 ms per 20k signals on 4096 atoms); where
+// shared memory limits residency its spills only cost time.
+template <typename T, int W, int MODE = -1>
+__global__ void __launch_bounds__(W * 32, 32 / W) lars_cta_kernel_lb(const LarsArgs<T> a) {
+  lars_cta_body<T, W, MODE>(a);
+}
+
+// The build a launch uses: mode-specialised or generic, register-bounded
+// where that keeps more CTAs resident (the grid helper below makes the same
+// choice, so a persistent grid matches the residency of the kernel it runs).
+template <typename T, int W>
+static auto pick_kernel(bool penalty, size_t smem) {
+  auto k = penalty ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
+  if constexpr (sizeof(T) == 4)
+    k = more_resident(k, penalty ? lars_cta_kernel_lb<T, W, 2> : lars_cta_kernel_lb<T, W>,
+                      W * 32, smem);
+  return k;
+}
+
 template <typename T, int W>
 static cudaError_t launch_w(const LarsArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-  auto k = (a.mode == 2 && !a.pos) ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
+  auto k = pick_kernel<T, W>(a.mode == 2 && !a.pos, smem);
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
@@ -458,7 +478,7 @@ size_t lars_cta_gstate_bytes(int Lc, int grid) {
 
 template <typename T, int W>
 static int grid_w(size_t smem, bool penalty) {
-  auto k = penalty ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
+  auto k = pick_kernel<T, W>(penalty, smem);
   int grid = 0;
   if (allow_smem(k, smem) != cudaSuccess || fill_grid(k, W * 32, smem, &grid) != cudaSuccess)
     return 0;

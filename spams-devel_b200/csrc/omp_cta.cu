@@ -23,13 +23,8 @@ __host__ __device__ inline size_t omp_cta_smem(int Kp, int Lc, size_t esz, int W
          (gstate ? 0 : omp_cta_state(Lc, esz));
 }
 
-// Single precision: at most 64 registers, so that up to 32 warps per SM are
-// resident (the per-step Gram-column reads from L2 need the parallelism:
-// 1.86 -> 1.40 ms per 20k signals of 18-step OMP on 1024 atoms, 5.87 -> 5.15
-// on 4096).
 template <typename T, int W>
-__global__ void __launch_bounds__(W * 32, sizeof(T) == 4 ? 32 / W : 1)
-omp_cta_kernel(const OmpArgs<T> a) {
+__device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
   constexpr int NV = 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -239,8 +234,24 @@ omp_cta_kernel(const OmpArgs<T> a) {
 }
 
 template <typename T, int W>
+__global__ void __launch_bounds__(W * 32) omp_cta_kernel(const OmpArgs<T> a) {
+  omp_cta_body<T, W>(a);
+}
+// The same kernel built with at most 64 registers, so that up to 32 warps per
+// SM can be resident (the per-step Gram-column reads from L2 need the
+// parallelism).  The launcher takes it only where it raises residency, i.e.
+// where shared memory is not the limit (small active-set capacity): 1.86 ->
+// 1.40 ms per 20k signals of 18-step OMP on 1024 atoms, 5.87 -> 5.15 on 4096;
+// with an 80-atom state it fits no more CTAs and its spills cost 5%.
+template <typename T, int W>
+__global__ void __launch_bounds__(W * 32, 32 / W) omp_cta_kernel_lb(const OmpArgs<T> a) {
+  omp_cta_body<T, W>(a);
+}
+
+template <typename T, int W>
 static cudaError_t launch_w(const OmpArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
   auto k = omp_cta_kernel<T, W>;
+  if constexpr (sizeof(T) == 4) k = more_resident(k, omp_cta_kernel_lb<T, W>, W * 32, smem);
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
