@@ -440,7 +440,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   const bool refac = p.lars && sizeof(T) == 4 && p.refactor != 0;
   if (refac)
     for (Shape& sh : cands)
-      if (sh.cta) sh.grid = lars_cta_grid<T>(Kp, sh.Lcap, false, p.mode == 2 && !p.pos);
+      if (sh.cta) sh.grid = lars_cta_grid<T>(Kp, sh.Lcap, false);
   const bool piped = sink && p.hX && !p.hmask;
   const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB

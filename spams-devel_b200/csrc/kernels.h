@@ -120,10 +120,9 @@ template <typename T>
 size_t lars_cta_smem_bytes(int Kp, int Lc, bool gstate);
 template <typename T>
 size_t lars_cta_gstate_bytes(int Lc, int grid);
-// The persistent grid the CTA launcher fills the device with (0 on error);
-// penalty: the PENALTY-without-pos instantiation (mode 2, pos 0).
+// The persistent grid the CTA launcher fills the device with (0 on error).
 template <typename T>
-int lars_cta_grid(int Kp, int Lc, bool gstate, bool penalty);
+int lars_cta_grid(int Kp, int Lc, bool gstate);
 
 template <typename T>
 cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);

@@ -48,9 +48,7 @@ __host__ __device__ inline size_t lars_cta_smem(int Kp, int Lc, size_t esz, int 
          (gstate ? 0 : lars_cta_state(Lc, esz));
 }
 
-// MODE >= 0 fixes the constraint mode at compile time (PENALTY without pos
-// prunes the other modes' code); -1 reads it from a.
-template <typename T, int W, int MODE>
+template <typename T, int W>
 __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   constexpr int NV = 4;  // 128-row chunks per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -81,8 +79,8 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   const T INF = inf<T>();
   const int L = a.L < K ? a.L : K;
   const int length_path = a.length_path <= 1 ? 4 * L : a.length_path;
-  const int mode = MODE >= 0 ? MODE : a.mode;
-  const bool pos = MODE >= 0 ? false : a.pos != 0;
+  const int mode = a.mode;
+  const bool pos = a.pos != 0;
   const int n_jobs = a.n_jobs_dev ? *a.n_jobs_dev : a.n_jobs;
   const int rbase = gw * NV * 128;
 
@@ -432,33 +430,33 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   }
 }
 
-template <typename T, int W, int MODE = -1>
+template <typename T, int W>
 __global__ void __launch_bounds__(W * 32) lars_cta_kernel(const LarsArgs<T> a) {
-  lars_cta_body<T, W, MODE>(a);
+  lars_cta_body<T, W>(a);
 }
 // The same kernel built with at most 64 registers, taken only where it keeps
 // more CTAs resident (2.57 -> 2.34 ms per 20k signals on 4096 atoms); where
 // shared memory limits residency its spills only cost time.
-template <typename T, int W, int MODE = -1>
+template <typename T, int W>
 __global__ void __launch_bounds__(W * 32, 32 / W) lars_cta_kernel_lb(const LarsArgs<T> a) {
-  lars_cta_body<T, W, MODE>(a);
+  lars_cta_body<T, W>(a);
 }
 
-// The build a launch uses: mode-specialised or generic, register-bounded
-// where that keeps more CTAs resident (the grid helper below makes the same
-// choice, so a persistent grid matches the residency of the kernel it runs).
+// The build a launch uses: register-bounded where that keeps more CTAs
+// resident (the grid helper below makes the same choice, so a persistent grid
+// matches the residency of the kernel it runs).  Unlike the warp kernel, this
+// one has no constraint-mode specialisation: a PENALTY-only build ran slower
+// (1.22 -> 1.47 ms per 1024-signal minibatch on 1024 atoms).
 template <typename T, int W>
-static auto pick_kernel(bool penalty, size_t smem) {
-  auto k = penalty ? lars_cta_kernel<T, W, 2> : lars_cta_kernel<T, W>;
-  if constexpr (sizeof(T) == 4)
-    k = more_resident(k, penalty ? lars_cta_kernel_lb<T, W, 2> : lars_cta_kernel_lb<T, W>,
-                      W * 32, smem);
+static auto pick_kernel(size_t smem) {
+  auto k = lars_cta_kernel<T, W>;
+  if constexpr (sizeof(T) == 4) k = more_resident(k, lars_cta_kernel_lb<T, W>, W * 32, smem);
   return k;
 }
 
 template <typename T, int W>
 static cudaError_t launch_w(const LarsArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-  auto k = pick_kernel<T, W>(a.mode == 2 && !a.pos, smem);
+  auto k = pick_kernel<T, W>(smem);
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);
@@ -477,8 +475,8 @@ size_t lars_cta_gstate_bytes(int Lc, int grid) {
 }
 
 template <typename T, int W>
-static int grid_w(size_t smem, bool penalty) {
-  auto k = pick_kernel<T, W>(penalty, smem);
+static int grid_w(size_t smem) {
+  auto k = pick_kernel<T, W>(smem);
   int grid = 0;
   if (allow_smem(k, smem) != cudaSuccess || fill_grid(k, W * 32, smem, &grid) != cudaSuccess)
     return 0;
@@ -486,17 +484,17 @@ static int grid_w(size_t smem, bool penalty) {
 }
 
 template <typename T>
-int lars_cta_grid(int Kp, int Lc, bool gstate, bool penalty) {
+int lars_cta_grid(int Kp, int Lc, bool gstate) {
   const size_t smem = lars_cta_smem_bytes<T>(Kp, Lc, gstate);
   switch (Kp / 512) {
-    case 1: return grid_w<T, 1>(smem, penalty);
-    case 2: return grid_w<T, 2>(smem, penalty);
-    case 3: return grid_w<T, 3>(smem, penalty);
-    case 4: return grid_w<T, 4>(smem, penalty);
-    case 5: return grid_w<T, 5>(smem, penalty);
-    case 6: return grid_w<T, 6>(smem, penalty);
-    case 7: return grid_w<T, 7>(smem, penalty);
-    case 8: return grid_w<T, 8>(smem, penalty);
+    case 1: return grid_w<T, 1>(smem);
+    case 2: return grid_w<T, 2>(smem);
+    case 3: return grid_w<T, 3>(smem);
+    case 4: return grid_w<T, 4>(smem);
+    case 5: return grid_w<T, 5>(smem);
+    case 6: return grid_w<T, 6>(smem);
+    case 7: return grid_w<T, 7>(smem);
+    case 8: return grid_w<T, 8>(smem);
     default: return 0;
   }
 }
@@ -522,8 +520,8 @@ template size_t lars_cta_smem_bytes<float>(int, int, bool);
 template size_t lars_cta_smem_bytes<double>(int, int, bool);
 template size_t lars_cta_gstate_bytes<float>(int, int);
 template size_t lars_cta_gstate_bytes<double>(int, int);
-template int lars_cta_grid<float>(int, int, bool, bool);
-template int lars_cta_grid<double>(int, int, bool, bool);
+template int lars_cta_grid<float>(int, int, bool);
+template int lars_cta_grid<double>(int, int, bool);
 template cudaError_t launch_lars_cta<float>(const LarsArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_lars_cta<double>(const LarsArgs<double>&, int, cudaStream_t);
 
