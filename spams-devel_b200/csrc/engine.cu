@@ -21,6 +21,7 @@
 #include "../../include/spams_b200.h"
 #include "engine.h"
 #include "kernels.h"
+#include "shape_plan.h"
 #include "refactor.cuh"
 
 namespace sc {
@@ -231,87 +232,32 @@ void profile_reset() { prof_reset(); }
 
 // Blocks of the refinement pass for active sets beyond 32 atoms.
 constexpr int kRefineBigGrid = 32;
-// Largest padded atom count of the warp-per-signal kernels, and of the
-// CTA-per-signal ones.
-constexpr int kWarpMaxKp = 1024;
-constexpr int kCtaMaxKp = 4096;
-
 // ---------------------------------------------------------------------------
 // launch shapes and their autotuner
 //
-// A signal is coded either by one warp (Kp <= 1024; its correlations in that
-// warp's registers) or by one CTA of Kp / 512 warps (Kp a multiple of 512).
-// Both run the same arithmetic in the same order, so they give the same bits;
-// they differ in speed: the warp kernel packs more signals per SM, the CTA
-// kernel holds larger active sets in shared memory and codes each signal
-// with more threads (lower latency when the batch is small or the active
-// sets outgrow the warp's capacity and take the overflow rerun).  The first
-// call of each (algorithm, precision, Kp, L class, batch-size class) times every
-// candidate on its first chunk and keeps the fastest; SC_AUTOTUNE=0 in the
-// environment selects the static rule instead (warp up to 1024 atoms).
-struct Shape {
-  bool cta;   // one CTA per signal
-  int Lcap;   // active-set capacity in shared memory
-  int wpb;    // warps per block (warp kernels) / per signal (CTA kernels)
-  int grid;   // persistent blocks (0: filled by the CTA launcher)
-};
-
+// The candidate shapes (shape_plan.h; kWarpMaxKp / kCtaMaxKp there are the
+// largest padded atom counts of the warp- and CTA-per-signal kernels) for
+// this device and the kernels' state sizes.  The first call of each
+// (algorithm, precision, Kp, L class, batch-size class) times every candidate
+// on its first chunk and keeps the fastest (pick_fastest); SC_AUTOTUNE=0 in
+// the environment selects the static rule instead (warp kernel up to 1024
+// atoms).
 template <typename T>
-static Shape warp_shape(const DeviceCtx& c, bool lars, int Kp, int L, int cap) {
-  Shape s;
-  s.cta = false;
-  s.Lcap = std::max(1, std::min(L, cap));
-  s.wpb = 8;
-  const size_t per_warp = lars ? lars_state_bytes(Kp, s.Lcap, sizeof(T))
-                               : omp_state_bytes(Kp, s.Lcap, sizeof(T));
-  while (s.wpb > 1 && (size_t)s.wpb * per_warp > (size_t)c.smem_per_block) s.wpb >>= 1;
-  const size_t per_block = (size_t)s.wpb * per_warp + 1024;
-  int bps = (int)((size_t)c.smem_per_sm / per_block);
-  const int regw = lars ? lars_max_warps_per_sm<T>(Kp) : omp_max_warps_per_sm<T>(Kp);
-  bps = std::min(bps, std::max(1, regw / s.wpb));
-  bps = std::max(1, std::min(bps, 64 / s.wpb));
-  s.grid = c.num_sms * bps;
-  return s;
-}
-
-template <typename T>
-static Shape cta_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
-  Shape s;
-  s.cta = true;
-  s.wpb = Kp / 512;
-  s.grid = 0;
-  // the small state is per CTA, so it can hold more atoms; keep two CTAs per
-  // SM within the shared-memory budget
+static std::vector<Shape> candidates_for(const DeviceCtx& c, bool lars, int Kp, int L,
+                                         int kernel) {
+  DeviceLimits d;
+  d.num_sms = c.num_sms;
+  d.smem_per_block = (size_t)c.smem_per_block;
+  d.smem_per_sm = (size_t)c.smem_per_sm;
+  auto state = [&](int lc) {
+    return lars ? lars_state_bytes(Kp, lc, sizeof(T)) : omp_state_bytes(Kp, lc, sizeof(T));
+  };
   auto bytes = [&](int lc) {
     return lars ? lars_cta_smem_bytes<T>(Kp, lc, false) : omp_cta_smem_bytes<T>(Kp, lc, false);
   };
-  s.Lcap = std::max(1, std::min(L, 80));
-  while (s.Lcap > 16 && (bytes(s.Lcap) > (size_t)c.smem_per_block ||
-                         2 * (bytes(s.Lcap) + 1024) > (size_t)c.smem_per_sm))
-    s.Lcap -= 16;
-  return s;
-}
-
-// The static rule: warp kernel up to kWarpMaxKp atoms, CTA kernel beyond.
-template <typename T>
-static Shape pick_shape(const DeviceCtx& c, bool lars, int Kp, int L) {
-  return Kp > kWarpMaxKp ? cta_shape<T>(c, lars, Kp, L) : warp_shape<T>(c, lars, Kp, L, 32);
-}
-
-// Every shape the layout Kp admits (the first one is the static rule's);
-// `kernel` (SC_KERNEL_*) keeps only one family.
-template <typename T>
-static std::vector<Shape> shape_candidates(const DeviceCtx& c, bool lars, int Kp, int L,
-                                           int kernel) {
-  std::vector<Shape> v;
-  const bool warp_ok = Kp <= kWarpMaxKp, cta_ok = Kp % 512 == 0 && Kp / 512 <= 8;
-  if (warp_ok && kernel != SC_KERNEL_CTA) {
-    v.push_back(warp_shape<T>(c, lars, Kp, L, 32));
-    if (L > 32) v.push_back(warp_shape<T>(c, lars, Kp, L, 64));
-  }
-  if (cta_ok && kernel != SC_KERNEL_WARP) v.push_back(cta_shape<T>(c, lars, Kp, L));
-  if (v.empty()) v.push_back(pick_shape<T>(c, lars, Kp, L));
-  return v;
+  const int regw = Kp > kWarpMaxKp ? 0
+                   : (lars ? lars_max_warps_per_sm<T>(Kp) : omp_max_warps_per_sm<T>(Kp));
+  return shape_candidates(d, Kp, L, kernel, state, regw, bytes);
 }
 
 struct TuneKey {
@@ -323,10 +269,6 @@ struct TuneKey {
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, int> g_tune;  // key -> index into shape_candidates
-
-// A candidate replaces the one kept so far only below this fraction of its
-// sample time.
-constexpr float kTuneMargin = 0.95f;
 
 static bool autotune_enabled() {
   static const bool on = [] {
@@ -434,7 +376,7 @@ template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
-  std::vector<Shape> cands = shape_candidates<T>(c, p.lars, Kp, p.L, p.kernel);
+  std::vector<Shape> cands = candidates_for<T>(c, p.lars, Kp, p.L, p.kernel);
   // FP64 refactor of single-precision LARS: one 16 KB scratch per warp (warp
   // kernels) or CTA (CTA kernels, whose grid is then fixed here)
   const bool refac = p.lars && sizeof(T) == 4 && p.refactor != 0;
@@ -598,10 +540,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // kernel family: a single candidate, the cached choice of an earlier call,
   // the static rule, or timed on the first chunk (tune)
   int chosen = cands.size() == 1 ? 0 : -1;
-  // L enters by class only (the candidate shapes differ at 32 and 64 atoms):
-  // a serving stream's batches carry many different L
-  const int lclass = p.L <= 32 ? 0 : (p.L <= 64 ? 1 : 2);
-  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, lclass, 0, p.kernel};
+  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, tune_lclass(p.L), 0, p.kernel};
   {
     int64_t c0 = std::min<int64_t>(nc, p.n), cls = 0;
     while (c0 > 1) { c0 >>= 1; ++cls; }
@@ -645,12 +584,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (stt != SC_OK) return stt;
-    // the static rule's shape (candidate 0) is kept unless another one is
-    // clearly faster on the sample: near-ties decided by timing noise made
-    // the choice, and so the full-batch speed, vary from run to run
-    int best = 0;
-    for (size_t i = 1; i < cands.size(); ++i)
-      if (t[i] < t[(size_t)best] * kTuneMargin) best = (int)i;
+    const int best = pick_fastest(t);  // the static rule's shape unless clearly beaten
     out = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;

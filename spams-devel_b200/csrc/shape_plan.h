@@ -1,0 +1,115 @@
+// Launch-shape planning for the coding kernels and the autotuner's choice
+// rule, as plain C++ (no CUDA calls) so that the arithmetic is unit-tested on
+// the CPU (tests/cpp/shape_plan_test.cpp).  No counterpart in the reference,
+// whose coding loops run one signal per OpenMP thread.
+//
+// A signal is coded either by one warp (Kp <= kWarpMaxKp; its correlations in
+// that warp's registers) or by one CTA of Kp / 512 warps (Kp a multiple of
+// 512).  Both run the same arithmetic in the same order, so they give the same
+// bits; they differ in speed: the warp kernel packs more signals per SM, the
+// CTA kernel holds larger active sets in shared memory and codes each signal
+// with more threads (lower latency when the batch is small or the active sets
+// outgrow the warp's capacity and take the overflow rerun).
+#pragma once
+#include <algorithm>
+#include <cstddef>
+#include <vector>
+
+#include "spams_b200.h"
+
+namespace sc {
+
+constexpr int kWarpMaxKp = 1024;
+constexpr int kCtaMaxKp = 4096;
+
+struct Shape {
+  bool cta = false;  // one CTA per signal
+  int Lcap = 0;      // active-set capacity in shared memory
+  int wpb = 0;       // warps per block (warp kernels) / per signal (CTA kernels)
+  int grid = 0;      // persistent blocks (0: filled by the CTA launcher)
+};
+
+// What the device offers a launch.
+struct DeviceLimits {
+  int num_sms = 0;
+  size_t smem_per_block = 0;  // opt-in dynamic shared memory per block
+  size_t smem_per_sm = 0;
+};
+
+// Warp kernel with an active-set capacity of at most `cap` atoms.
+// state(lc): one warp's shared-memory state for capacity lc; regw: the warps
+// per SM the kernel's registers allow.  Blocks of up to 8 warps (fewer when a
+// block's state would not fit), as many blocks per SM as shared memory (1 KB
+// reserved per block), registers and the 64-warp limit allow.
+template <typename StateBytes>
+inline Shape warp_shape(const DeviceLimits& d, int L, int cap, StateBytes state, int regw) {
+  Shape s;
+  s.cta = false;
+  s.Lcap = std::max(1, std::min(L, cap));
+  s.wpb = 8;
+  const size_t per_warp = state(s.Lcap);
+  while (s.wpb > 1 && (size_t)s.wpb * per_warp > d.smem_per_block) s.wpb >>= 1;
+  const size_t per_block = (size_t)s.wpb * per_warp + 1024;
+  int bps = (int)(d.smem_per_sm / per_block);
+  bps = std::min(bps, std::max(1, regw / s.wpb));
+  bps = std::max(1, std::min(bps, 64 / s.wpb));
+  s.grid = d.num_sms * bps;
+  return s;
+}
+
+// CTA kernel: the small state is per CTA, so it can hold more atoms (up to
+// 80); the capacity shrinks in steps of 16 until two CTAs fit per SM.
+// bytes(lc): one CTA's shared memory for capacity lc.
+template <typename CtaBytes>
+inline Shape cta_shape(const DeviceLimits& d, int Kp, int L, CtaBytes bytes) {
+  Shape s;
+  s.cta = true;
+  s.wpb = Kp / 512;
+  s.grid = 0;
+  s.Lcap = std::max(1, std::min(L, 80));
+  while (s.Lcap > 16 &&
+         (bytes(s.Lcap) > d.smem_per_block || 2 * (bytes(s.Lcap) + 1024) > d.smem_per_sm))
+    s.Lcap -= 16;
+  return s;
+}
+
+// Every shape the layout Kp admits, the static rule's first (warp kernel up
+// to kWarpMaxKp atoms with a 32-atom state, CTA kernel beyond): the warp
+// kernel with a 32- and, when L > 32, a 64-atom state, and the CTA kernel;
+// `kernel` (SC_KERNEL_*) keeps only one family.
+template <typename WarpState, typename CtaBytes>
+inline std::vector<Shape> shape_candidates(const DeviceLimits& d, int Kp, int L, int kernel,
+                                           WarpState state, int regw, CtaBytes bytes) {
+  std::vector<Shape> v;
+  const bool warp_ok = Kp <= kWarpMaxKp, cta_ok = Kp % 512 == 0 && Kp / 512 <= 8;
+  if (warp_ok && kernel != SC_KERNEL_CTA) {
+    v.push_back(warp_shape(d, L, 32, state, regw));
+    if (L > 32) v.push_back(warp_shape(d, L, 64, state, regw));
+  }
+  if (cta_ok && kernel != SC_KERNEL_WARP) v.push_back(cta_shape(d, Kp, L, bytes));
+  if (v.empty())
+    v.push_back(Kp > kWarpMaxKp ? cta_shape(d, Kp, L, bytes) : warp_shape(d, L, 32, state, regw));
+  return v;
+}
+
+// The autotuner keys its choice by L only through this class: the candidate
+// shapes differ at 32 and 64 atoms, and a serving stream's batches carry many
+// different L.
+inline int tune_lclass(int L) { return L <= 32 ? 0 : (L <= 64 ? 1 : 2); }
+
+// A candidate replaces the one kept so far only below this fraction of its
+// sample time.
+constexpr float kTuneMargin = 0.95f;
+
+// The autotuner's pick from the candidates' sample times (the static rule's
+// shape first): another shape replaces the one kept so far only when clearly
+// faster, since near-ties decided by timing noise made the choice, and so
+// the full-batch speed, vary from run to run.
+inline int pick_fastest(const std::vector<float>& t, float margin = kTuneMargin) {
+  int best = 0;
+  for (size_t i = 1; i < t.size(); ++i)
+    if (t[i] < t[(size_t)best] * margin) best = (int)i;
+  return best;
+}
+
+}  // namespace sc
