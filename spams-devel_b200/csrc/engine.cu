@@ -359,18 +359,10 @@ struct HostSink {
   }
 };
 
-// Host-array calls code their signals in chunks of about n / kPipeChunks
-// (at least kPipeMinChunk signals) after a first chunk half that size: while
-// one chunk is coded, the next one is copied in on the H2D stream and the
-// previous chunk's CSC is read back.  The result arrays are sized after the
-// first chunk from its entries per signal (one allocation instead of a
-// growing series of reallocations and copies).  Measured on the 100k-signal
-// lasso workload: 3.31 ms end to end against 3.36 with a quarter-size first
-// chunk and growth by reallocation, 3.30-3.94 ms for 3 to 8 chunks; a second
-// coding stream for alternate chunks was slower.
-constexpr int kPipeChunks = 5;
-constexpr int64_t kPipeMinChunk = 16384;
-constexpr int64_t kPipeFirstDiv = 2;
+// Host-array calls code their signals in chunks (chunk_signals / plan_chunks,
+// shape_plan.h).  The result arrays are sized after the first chunk from its
+// entries per signal (one allocation instead of a growing series of
+// reallocations and copies).
 
 template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
@@ -390,13 +382,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                          (p.hX ? (size_t)nbuf * p.m * sizeof(T) : 0) +
                          (p.tc ? (size_t)p.mp * 4 : 0) +
                          (sink ? (size_t)nbuf * (p.L * (sizeof(T) + 4) + 8) : 0);
-  int64_t nc = (int64_t)std::max<size_t>(4096, ((size_t)2 << 30) / per_sig);
-  nc = std::min<int64_t>(nc, std::max<int64_t>(p.n, 1));
-  nc = std::min<int64_t>(nc, (int64_t)1 << 30);
-  if (piped) {
-    const int64_t k = std::max<int64_t>(1, std::min<int64_t>(kPipeChunks, p.n / kPipeMinChunk));
-    nc = std::min<int64_t>(nc, (p.n + k - 1) / k);
-  }
+  const int64_t nc = chunk_signals(p.n, per_sig, piped);
 
   SC_TRY(c.dtx.reserve((size_t)Kp * nc * sizeof(T)));
   SC_TRY(c.norms.reserve((size_t)nc * sizeof(T)));
@@ -483,16 +469,11 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
   g_prof.signals += p.n;
 
-  // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i)).
-  // With the pipeline the first chunk is 1/kPipeFirstDiv of the others: its
-  // copy-in is the only one nothing overlaps.
-  const int64_t first = piped ? std::max<int64_t>(1, std::min<int64_t>(p.n, nc / kPipeFirstDiv)) : nc;
-  const int64_t nchunks =
-      p.n <= 0 ? 0 : (p.n <= first ? 1 : 1 + (p.n - first + nc - 1) / nc);
-  auto chunk_start = [&](int64_t i) { return i == 0 ? (int64_t)0 : first + (i - 1) * nc; };
-  auto chunk_len = [&](int64_t i) {
-    return std::min<int64_t>(i == 0 ? first : nc, p.n - chunk_start(i));
-  };
+  // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i))
+  const ChunkPlan plan = plan_chunks(p.n, nc, piped);
+  const int64_t nchunks = plan.count;
+  auto chunk_start = [&](int64_t i) { return plan.start(i); };
+  auto chunk_len = [&](int64_t i) { return plan.len(i); };
   auto xslot_ptr = [&](int64_t i) {
     return reinterpret_cast<T*>(static_cast<char*>(c.xstage.ptr) + (i & 1) * (piped ? xslot : 0));
   };

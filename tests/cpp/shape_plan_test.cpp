@@ -111,6 +111,55 @@ int main() {
   CHECK(pick_fastest({1.0f, 0.90f, 0.85f}) == 2);
   CHECK(pick_fastest({1.0f, 2.0f, 0.5f}) == 2);
 
+  // host-array chunking: contiguous chunks covering [0, n), the first one half
+  // the others with the copy pipeline
+  auto covers = [](const ChunkPlan& c) {
+    int64_t at = 0;
+    for (int64_t i = 0; i < c.count; ++i) {
+      if (c.start(i) != at || c.len(i) <= 0) return false;
+      at += c.len(i);
+    }
+    return at == c.n;
+  };
+  {
+    // the 100k-signal lasso workload's host call (Kp 512, L 256, m 256, BF16 split)
+    const size_t per_sig = 512 * 4 + 256 * 8 + 64 + 2 * 256 * 4 + 256 * 4 + 2 * (256 * 8 + 8);
+    const int64_t nc = chunk_signals(100000, per_sig, true);
+    CHECK(nc == 20000);
+    const ChunkPlan c = plan_chunks(100000, nc, true);
+    CHECK(c.count == 6 && c.first == 10000 && covers(c));
+    CHECK(c.len(1) == 20000 && c.len(4) == 20000 && c.len(5) == 10000);
+  }
+  {
+    // without the pipeline: one chunk up to the ~2 GiB buffer bound
+    const int64_t nc = chunk_signals(100000, 8192, false);
+    CHECK(nc == 100000);
+    ChunkPlan c = plan_chunks(100000, nc, false);
+    CHECK(c.count == 1 && covers(c));
+    const int64_t big = chunk_signals(1000000, 8192, false);
+    CHECK(big == ((int64_t)2 << 30) / 8192);
+    c = plan_chunks(1000000, big, false);
+    CHECK(c.count == 4 && covers(c));
+  }
+  {
+    // small host calls: one chunk of everything (fewer than 2 x 16384 signals)
+    const int64_t nc = chunk_signals(20000, 4096, true);
+    CHECK(nc == 20000);
+    const ChunkPlan c = plan_chunks(20000, nc, true);
+    CHECK(c.first == 10000 && c.count == 2 && covers(c));
+    CHECK(plan_chunks(1, chunk_signals(1, 4096, true), true).count == 1);
+    CHECK(plan_chunks(0, chunk_signals(0, 4096, true), true).count == 0);
+  }
+  for (int64_t n : {16384, 50000, 99999, 100001, 1000000, 3333333}) {
+    const int64_t nc = chunk_signals(n, 4096, true);
+    const ChunkPlan c = plan_chunks(n, nc, true);
+    CHECK(covers(c) && c.first == std::max<int64_t>(1, nc / kPipeFirstDiv));
+    // at most kPipeChunks full chunks unless the buffer bound (2 GiB / 4096 B)
+    // makes them smaller
+    if (nc < ((int64_t)2 << 30) / 4096) CHECK(c.count <= kPipeChunks + 1);
+    else CHECK(nc == ((int64_t)2 << 30) / 4096);
+  }
+
   if (failures) {
     std::printf("%d check(s) failed\n", failures);
     return 1;
