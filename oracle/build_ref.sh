@@ -10,10 +10,13 @@
 # "scipy_" prefix; a generated forced-include header renames each symbol.
 # The ILP64 numpy OpenBLAS must not be used: the reference's INTT is int.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_DIR]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_DIR]
+#   REFERENCE_DIR: the argument, else $SPAMS_REFERENCE_DIR, else the read-only
+#   checkout this recipe was written against (/root/reference).  Exits 2 when
+#   no reference sources are found there.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${SPAMS_REFERENCE_DIR:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/decomp" ]; then
   echo "build_ref: reference sources not found at $REF" >&2

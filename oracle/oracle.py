@@ -22,7 +22,8 @@ import scipy.sparse as ssp
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_SO = os.path.join(HERE, "liborc.so")
 REF_SO = os.path.join(HERE, "_ref", "libspams_ref.so")
-REFERENCE_DIR = "/root/reference"
+# The reference checkout: SPAMS_REFERENCE_DIR, else build_ref.sh's own default.
+REFERENCE_DIR = os.environ.get("SPAMS_REFERENCE_DIR")
 
 
 def build_orc() -> str:
@@ -33,16 +34,23 @@ def build_orc() -> str:
     return ORC_SO
 
 
-def build_ref(reference_dir: str = REFERENCE_DIR) -> str | None:
-    """Compile oracle/_ref from the reference sources when they are present."""
+def build_ref(reference_dir: str | None = REFERENCE_DIR) -> str | None:
+    """Compile oracle/_ref from the reference sources when they are present.
+
+    ``reference_dir`` (or SPAMS_REFERENCE_DIR) names the checkout; without it
+    build_ref.sh looks in its own default location.  The script exits 2 when
+    it finds no sources, and an existing build is then kept as it is.
+    """
     deps = [os.path.join(HERE, "ref_driver.cpp"), os.path.join(HERE, "build_ref.sh")]
     fresh = os.path.exists(REF_SO) and all(os.path.getmtime(d) <= os.path.getmtime(REF_SO) for d in deps)
     if fresh:
         return REF_SO
-    if not os.path.isdir(os.path.join(reference_dir, "decomp")):
+    cmd = ["bash", os.path.join(HERE, "build_ref.sh")] + ([reference_dir] if reference_dir else [])
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode == 2:
         return REF_SO if os.path.exists(REF_SO) else None
-    subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_dir], check=True,
-                   capture_output=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build_ref.sh failed:\n{r.stderr[-2000:]}")
     return REF_SO
 
 

@@ -2,10 +2,15 @@
 
     python spams-devel_b200/build.py [--jobs N] [--verbose]
 
-Every CUDA source under csrc/ is compiled for sm_100a only
+The CUDA sources listed in SOURCES are compiled for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) and linked, with the C ABI of
 include/spams_b200.h, into spams-devel_b200/lib/libspams_b200.so.  Object files
 go to spams-devel_b200/_build/.  Rebuilds only what changed.
+
+The list is explicit: a stray .cu file in csrc/ is an error, not a silent
+part of the library.  Before linking, the weak (template-instantiation) host
+symbols of every object are compared: two objects that define the same one
+would let the linker keep whichever comes first, so that is an error too.
 """
 from __future__ import annotations
 
@@ -35,8 +40,53 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+SOURCES = [
+    "csc.cu", "dl.cu", "engine.cu", "gemm.cu", "lars.cu", "lars_cta.cu", "mask.cu",
+    "noalloc.cu", "omp.cu", "omp_cta.cu", "refine.cu", "serve.cu", "tc_gemm.cu",
+]
+
+
 def sources() -> list[str]:
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    present = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    extra = sorted(set(present) - set(SOURCES))
+    missing = sorted(set(SOURCES) - set(present))
+    if extra or missing:
+        raise RuntimeError(f"csrc/ does not match the source list: unlisted {extra}, missing {missing}")
+    return [os.path.join(CSRC, f) for f in SOURCES]
+
+
+def _weak_host_symbols(obj: str) -> set[str]:
+    """Defined weak symbols of one object's host code (nm types W/V)."""
+    r = subprocess.run(["nm", "--defined-only", obj], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nm failed on {obj}: {r.stderr}")
+    out = set()
+    for line in r.stdout.splitlines():
+        parts = line.split()
+        if len(parts) == 3 and parts[1] in ("W", "V"):
+            out.add(parts[2])
+    return out
+
+
+def check_duplicate_weak(objs: list[str]) -> None:
+    """Refuse a link in which two objects define the same project symbol weakly.
+
+    Project code lives in namespace ``sc`` (mangled ``_ZN2sc``); a weak ``sc::``
+    symbol in two objects means two explicit instantiations of the same
+    template, and the linker would keep one of them without a word.
+    """
+    seen: dict[str, str] = {}
+    dups = []
+    for o in objs:
+        for sym in _weak_host_symbols(o):
+            if not sym.startswith("_ZN2sc"):
+                continue
+            if sym in seen and seen[sym] != o:
+                dups.append((sym, os.path.basename(seen[sym]), os.path.basename(o)))
+            seen.setdefault(sym, o)
+    if dups:
+        lines = "\n".join(f"  {s} in {a} and {b}" for s, a, b in dups[:20])
+        raise RuntimeError(f"weak project symbols defined by two objects:\n{lines}")
 
 
 def headers() -> list[str]:
@@ -92,6 +142,7 @@ def build(jobs: int = 0, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     if _stale(LIB, objs):
+        check_duplicate_weak(objs)
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
