@@ -21,7 +21,14 @@ collective on the data path); rank 0 prints the aggregate.  `--impl
 reference` times the SPAMS reference's own CPU code (oracle/_ref) on the host
 cores instead.
 
-Two more workloads, each printing its own JSON line (one GPU):
+On one GPU the default line also carries the other benchmarked
+configurations as sub-objects, each with its own value, e2e, roofline and CPU
+baseline, at bounded sizes (the whole run takes a few minutes):
+  "uneven_omp" (2e5 signals, --uneven-n), "dictlearn" (2000 minibatches),
+  "serve" (2000 req/s for 5 s, then 1000 and 500 req/s); --no-sub-workloads
+  leaves them out.
+
+The same workloads at full size, each printing its own JSON line (one GPU):
   --workload uneven_omp  batched uneven OMP: D 512 x 2048, X 512 x 1e6,
                          s_i ~ U{1..64}, L_i = s_i + 4, eps_i = 0.5 ||noise_i||^2
   --workload serve       serving stream: Poisson arrivals at --rate req/s over
@@ -108,7 +115,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -375,6 +382,14 @@ def run_ours(args) -> None:
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
+    if world == 1 and not args.no_sub_workloads:
+        # the other benchmarked configurations, bounded to a few minutes in all
+        sub_cpu = min(args.cpu_seconds, 5.0)
+        line["uneven_omp"] = uneven_omp_result(args.uneven_n, 5, 3, args.precision, sub_cpu,
+                                               args.no_cpu_baseline)
+        line["dictlearn"] = dictlearn_result(2000, 3, args.precision, sub_cpu,
+                                             args.no_cpu_baseline)
+        line["serve"] = serve_result(2000.0, 5.0, args.slots, args.precision, (500.0, 1000.0))
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -388,14 +403,15 @@ UO_METRIC = ("coded signals/s (batched uneven OMP, D 512x2048, s~U{1..64}, L=s+4
              "eps=0.5||noise||^2)")
 
 
-def run_uneven_omp(args) -> None:
+def uneven_omp_result(n: int, steps: int, warmup: int, precision: str, cpu_seconds: float,
+                      no_cpu: bool = False) -> dict:
+    """The batched uneven OMP workload on n device-drawn signals."""
     import torch
     import spams_b200
     from spams_b200 import workloads as W
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
-    n = args.n or 1000000
+    prec = spams_b200.SC_PREC_BF16X3 if precision == "bf16x3" else spams_b200.SC_PREC_FP32
     X, D, Lv, eps = W.config_uneven_omp_device(n=n, seed=0, m=UO_M, K=UO_K, device=dev)
     Lmax = int(Lv.max().item())
     cap = n * Lmax
@@ -408,16 +424,16 @@ def run_uneven_omp(args) -> None:
         return spams_b200.omp_device(X, D, L=Lmax, L_vec=Lv, eps_vec=eps, stream=stream,
                                      precision=p, out=outs, sync=False, profile=profile)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    # inputs (2 GB of X, 8 GB of correlations per pass) exceed L2
+    # inputs (X and the correlations of a pass) exceed L2
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+           for _ in range(steps)]
     launches = 0
     with Clocks(0) as clk:
         torch.cuda.synchronize()
-        for i in range(args.steps):
+        for i in range(steps):
             evs[i][0].record(stream)
             step()
             evs[i][1].record(stream)
@@ -431,17 +447,13 @@ def run_uneven_omp(args) -> None:
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step(p=spams_b200.SC_PREC_FP32)
         e1.record(stream)
         torch.cuda.synchronize()
         fp32_ms = e0.elapsed_time(e1)
-    stage = {"ms_corr": 0.0, "ms_code": 0.0, "ms_csc": 0.0, "ms_norms": 0.0, "ms_gram": 0.0,
-             "ms_refine": 0.0, "steps": 0, "overflowed": 0}
     step(profile=True)
-    p = spams_b200.last_profile()
-    for k in stage:
-        stage[k] = p[k]
+    prof = spams_b200.last_profile()
     # end to end: host arrays (pinned) in, CSC on the host out
     Xh = torch.empty((n, UO_M), dtype=torch.float32, pin_memory=True)
     Xh.copy_(X.t())
@@ -450,13 +462,13 @@ def run_uneven_omp(args) -> None:
     Lnp, Enp = Lv.cpu().numpy(), eps.cpu().numpy()
     spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
     e2e_t = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(max(1, min(steps, 3))):
         t0 = time.perf_counter()
         a = spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_t) / len(e2e_t)
     cpu = None
-    if not args.no_cpu_baseline:
+    if not no_cpu:
         try:
             from oracle import oracle as O
             O.build_ref()
@@ -464,7 +476,7 @@ def run_uneven_omp(args) -> None:
             t0 = time.perf_counter()
             O.ref_omp(Xnp[:, :cal], Dnp, L=Lnp[:cal], eps=Enp[:cal], numThreads=-1)
             dt = max(time.perf_counter() - t0, 1e-6)
-            sample = int(min(n, max(cal, cal * args.cpu_seconds / dt)))
+            sample = int(min(n, max(cal, cal * cpu_seconds / dt)))
             t0 = time.perf_counter()
             O.ref_omp(np.asfortranarray(Xnp[:, :sample]), Dnp, L=Lnp[:sample], eps=Enp[:sample],
                       numThreads=-1)
@@ -477,37 +489,43 @@ def run_uneven_omp(args) -> None:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
     peaks = measured_peaks()
-    code_ms = stage["ms_code"]
+    code_ms = prof["ms_code"]
     # per signal: the K-float correlation column, one K-float Gram column per
     # selected atom, the (index, value) pair of each coefficient
-    alg_bytes = 4 * UO_K * n + 4 * UO_K * stage["steps"] + 8 * nnz
+    alg_bytes = 4 * UO_K * n + 4 * UO_K * prof["steps"] + 8 * nnz
     achieved = alg_bytes / (code_ms / 1e3) / 1e9 if code_ms > 0 else None
-    value = n * args.steps / (total_ms / 1e3)
-    line = {
-        "metric": UO_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+    kname = "omp_cta_kernel" if prof["kernel"] == spams_b200.SC_KERNEL_CTA else "omp_kernel"
+    value = n * steps / (total_ms / 1e3)
+    return {
+        "metric": UO_METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded, drawn on the device)",
         "config": {"workload": f"uneven_omp_D{UO_M}x{UO_K}_n{n}_s1-64_noise0.02",
-                   "m": UO_M, "K": UO_K, "n": n, "precision": args.precision,
-                   "between_steps": "inputs larger than L2 (2 GB of X)",
+                   "m": UO_M, "K": UO_K, "n": n, "precision": precision,
+                   "between_steps": "inputs larger than L2 (X and the correlations of a pass)",
                    "parallelism": "one GPU"},
         "e2e": {"value": n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Xnp.nbytes + Dnp.nbytes
                 + Lnp.nbytes + Enp.nbytes, "d2h_bytes_per_step": (n + 1) * 8 + a.nnz * 8},
         "gpu_launches": launches,
-        "roofline": {"kernel": "omp_cta_kernel", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
                      "traffic": None, "peak_source": peaks["source"],
-                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
-        "stages_ms": {k: stage[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
-                                            "ms_refine", "ms_csc")},
-        "fp32_value": (n * args.steps / (fp32_ms / 1e3)) if fp32_ms else value,
-        "omp_steps_per_signal": stage["steps"] / n, "nnz_per_signal": nnz / n,
-        "overflowed_signals": stage["overflowed"],
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms,
+                     "active_set_capacity": prof["lcap"]},
+        "stages_ms": {k: prof[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
+                                           "ms_refine", "ms_csc")},
+        "fp32_value": (n * steps / (fp32_ms / 1e3)) if fp32_ms else value,
+        "omp_steps_per_signal": prof["steps"] / n, "nnz_per_signal": nnz / n,
+        "overflowed_signals": prof["overflowed"],
         "clocks": clk.summary(), "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_uneven_omp(args) -> None:
+    print(json.dumps(uneven_omp_result(args.n or 1000000, args.steps, args.warmup, args.precision,
+                                       args.cpu_seconds, args.no_cpu_baseline)), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -542,31 +560,32 @@ def _serve_requests(pools, rate, duration, seed, prec):
     return recs, arrival, int(n.sum())
 
 
-def run_serve(args) -> None:
+def serve_result(rate: float, duration: float, slots: int, precision: str,
+                 sweep_rates=(250.0, 500.0, 1000.0)) -> dict:
+    """The serving stream at `rate` requests/s (then each lower rate of
+    sweep_rates), p50 / p99 latency from arrival to the result on the host."""
     import torch
     import spams_b200
     from spams_b200 import workloads as W
     torch.cuda.set_device(0)
-    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
+    prec = spams_b200.SC_PREC_BF16X3 if precision == "bf16x3" else spams_b200.SC_PREC_FP32
     dicts, pools, _ = W.config_serving(rate=1.0, duration_s=1.0, seed=0)
     pinned = []
     for P in pools:  # request signals live in pinned host memory
         h = torch.empty((P.shape[1], P.shape[0]), dtype=torch.float32, pin_memory=True)
         h.numpy()[:] = P.T
         pinned.append(h.numpy().T)
-    out = {}
-    with spams_b200.Server(hbm_budget=150e9, slots=args.slots) as srv:
+    with spams_b200.Server(hbm_budget=150e9, slots=slots) as srv:
         for i, D in enumerate(dicts):
             srv.add_dictionary(i, D)
         # warm-up: one second of the stream (kernels loaded, workspaces grown)
-        recs, arr, _ = _serve_requests(pinned, args.rate, 1.0, 99, prec)
+        recs, arr, _ = _serve_requests(pinned, rate, 1.0, 99, prec)
         srv.replay(recs, arr)
         sweep = []
-        rates = [args.rate] + ([r for r in (250.0, 500.0, 1000.0) if r < args.rate]
-                               if not args.no_sweep else [])
+        rates = [rate] + [r for r in sweep_rates if r < rate]
         clk_summary = None
-        for rate in rates:
-            recs, arr, offered = _serve_requests(pinned, rate, args.duration, int(rate), prec)
+        for r in rates:
+            recs, arr, offered = _serve_requests(pinned, r, duration, int(r), prec)
             srv.stats(reset=True)
             with Clocks(0) as clk:
                 t0 = time.perf_counter()
@@ -575,32 +594,37 @@ def run_serve(args) -> None:
             st = srv.stats(reset=True)
             if clk_summary is None:
                 clk_summary = clk.summary()
-            sweep.append({"rate_req_s": rate, "requests": len(recs),
-                          "offered_signals_s": offered / args.duration,
+            sweep.append({"rate_req_s": r, "requests": len(recs),
+                          "offered_signals_s": offered / duration,
                           "served_signals_s": st["signals"] / wall, "wall_s": wall,
                           "p50_ms": st["lat_p50_ms"], "p99_ms": st["lat_p99_ms"],
                           "mean_ms": st["lat_mean_ms"], "max_ms": st["lat_max_ms"],
                           "requests_per_launch": st["mean_batch_requests"],
                           "rejected": st["rejected"], "gpu_busy_s": st["busy_s"],
                           "peak_device_bytes": st["peak_device_bytes"]})
-        out = sweep[0]
-    line = {
+    out = sweep[0]
+    return {
         "metric": SERVE_METRIC, "value": out["p99_ms"], "unit": "ms", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": out["wall_s"] * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; signals drawn once into per-dictionary pools)",
-        "config": {"workload": f"serving_poisson{args.rate:g}rps_{args.duration:g}s",
-                   "dictionaries": [list(t) for t in W.SERVING_DICTS], "slots": args.slots,
-                   "hbm_budget_bytes": 150e9, "precision": args.precision,
+        "config": {"workload": f"serving_poisson{rate:g}rps_{duration:g}s",
+                   "dictionaries": [list(t) for t in W.SERVING_DICTS], "slots": slots,
+                   "hbm_budget_bytes": 150e9, "precision": precision,
                    "between_steps": "inputs larger than L2 (pools of 0.39 GB)",
                    "parallelism": "one GPU"},
-        "p50_ms": out["p50_ms"], "served_signals_s": out["served_signals_s"],
+        "rate_req_s": rate, "p50_ms": out["p50_ms"], "p99_ms": out["p99_ms"],
+        "served_signals_s": out["served_signals_s"],
         "offered_signals_s": out["offered_signals_s"],
         "e2e": {"value": out["p99_ms"], "unit": "ms", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None},
         "sweep": sweep, "clocks": clk_summary,
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_serve(args) -> None:
+    print(json.dumps(serve_result(args.rate, args.duration, args.slots, args.precision,
+                                  () if args.no_sweep else (250.0, 500.0, 1000.0))), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -612,20 +636,25 @@ DL_METRIC = ("minibatches/s (online dictionary-learning step: 1024 signals of 12
              "Lasso lambda1=0.1, A/B accumulations)")
 
 
-def run_dictlearn(args) -> None:
+def dictlearn_result(nb: int, warmup: int, precision: str, cpu_seconds: float,
+                     no_cpu: bool = False) -> dict:
+    """nb minibatches of the online dictionary-learning step, one CUDA-graph
+    replay each; e2e runs the same nb minibatches through the eager API with
+    each minibatch copied in from pinned host memory."""
     import torch
     import spams_b200
     from spams_b200 import workloads as W
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    prec = spams_b200.SC_PREC_BF16X3 if args.precision == "bf16x3" else spams_b200.SC_PREC_FP32
-    nb = args.n or 2000  # minibatches
+    prec = spams_b200.SC_PREC_BF16X3 if precision == "bf16x3" else spams_b200.SC_PREC_FP32
     rng = np.random.Generator(np.random.PCG64(0))
-    pool = 200000
+    nwin = 195
+    pool = nwin * DL_BATCH  # 199680 signals: minibatch i is window i mod 195 of the permutation
     Xnp = W.smooth_patches(pool, rng, side=12).astype(np.float32)
     D0 = Xnp[:, rng.choice(pool, DL_K, replace=False)]  # random signals, as train() starts
     D0 = np.asfortranarray(D0 / np.linalg.norm(D0, axis=0, keepdims=True))
-    perm = torch.from_numpy(rng.permutation(pool).astype(np.int32)).to(dev)
+    perm_np = rng.permutation(pool).astype(np.int32)
+    perm = torch.from_numpy(perm_np).to(dev)
     Xd = torch.from_numpy(np.ascontiguousarray(Xnp.T)).to(dev).t()
     U = torch.from_numpy(rng.standard_normal((DL_M, nb + 1)).astype(np.float32)).to(dev)
     V = torch.from_numpy(rng.standard_normal((DL_K, nb + 1)).astype(np.float32)).to(dev)
@@ -640,19 +669,21 @@ def run_dictlearn(args) -> None:
     step = spams_b200.MinibatchStep(DL_M, DL_K, DL_BATCH, lambda1=DL_LAMBDA, precision=prec)
     Dd, A, B, it = fresh()
 
-    def body():
-        # the dictionary changes every minibatch: rank-1 perturbation (the
-        # minibatch's column of U, V, picked by the device counter), unit columns
-        u = U.index_select(1, it).squeeze(1)
-        v = V.index_select(1, it).squeeze(1)
-        Dd.add_(0.01 * torch.outer(u, v))
+    def perturb(ui, vi):
+        # the dictionary changes every minibatch: rank-1 perturbation, then
+        # unit columns again
+        Dd.add_(0.01 * torch.outer(ui, vi))
         Dd.div_(Dd.norm(dim=0, keepdim=True))
+
+    def body():
+        # the minibatch's column of U and V is picked by the device counter
+        perturb(U.index_select(1, it).squeeze(1), V.index_select(1, it).squeeze(1))
         step(Dd, Xd, it, perm=perm, A=A, B=B, beta=1.0, gamma=1.0 / DL_BATCH)
 
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(s):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             body()
     torch.cuda.current_stream().wait_stream(s)
     torch.cuda.synchronize()
@@ -684,7 +715,7 @@ def run_dictlearn(args) -> None:
     e1.record()
     torch.cuda.synchronize()
     eager_ms = e0.elapsed_time(e1)
-    # ---- stage times of one eager step
+    # ---- stage times and launches of one eager step
     step.profile(True)
     body()
     torch.cuda.synchronize()
@@ -692,38 +723,43 @@ def run_dictlearn(args) -> None:
     step.profile(False)
     cp, rows, vals = step.codes()
     nnz = int(cp[-1].item())
-    # ---- end to end: each minibatch copied in from pinned host memory, its
-    # code count read back
-    Xh = torch.empty((DL_BATCH * 50, DL_M), dtype=torch.float32, pin_memory=True)
-    Xh.numpy()[:] = Xnp[:, :DL_BATCH * 50].T
+    # ---- end to end: the same nb minibatches, each copied in from pinned
+    # host memory (minibatch i = window i mod 195 of the permuted pool, the
+    # columns the graph loop reads), D perturbed and renormalised, coded and
+    # accumulated, its code count read back
+    Xh = torch.empty((pool, DL_M), dtype=torch.float32, pin_memory=True)
+    Xh.numpy()[:] = Xnp[:, perm_np].T
     Xbuf = torch.empty((DL_BATCH, DL_M), device=dev).t()
     it1 = torch.zeros(1, dtype=torch.int64, device=dev)
     Dd, A, B, it = fresh()
-    ne2 = 50
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for i in range(ne2):
-        Xbuf.copy_(Xh[i * DL_BATCH:(i + 1) * DL_BATCH].t(), non_blocking=True)
-        it1.zero_()
+    for i in range(nb):
+        w = i % nwin
+        Xbuf.copy_(Xh[w * DL_BATCH:(w + 1) * DL_BATCH].t(), non_blocking=True)
+        perturb(U[:, i], V[:, i])
         step(Dd, Xbuf, it1, A=A, B=B, beta=1.0, gamma=1.0 / DL_BATCH)
-        c2 = step.codes()[0]
-        int(c2[-1].item())
-    e2e_s = (time.perf_counter() - t0) / ne2
+        int(step.codes()[0][-1].item())
+    e2e_s = (time.perf_counter() - t0) / nb
     cpu = None
-    if not args.no_cpu_baseline:
+    if not no_cpu:
         try:
             from oracle import oracle as O
             O.build_ref()
-            Xb = np.asfortranarray(Xnp[:, :DL_BATCH])
+            Ah = np.zeros((DL_K, DL_K), np.float32, order="F")
+            Bh = np.zeros((DL_M, DL_K), np.float32, order="F")
             reps, t0 = 0, time.perf_counter()
-            while time.perf_counter() - t0 < args.cpu_seconds and reps < 200:
-                O.ref_lasso(Xb, D0, lambda1=DL_LAMBDA, L=min(DL_M, DL_K), numThreads=-1)
+            while time.perf_counter() - t0 < cpu_seconds and reps < 200:
+                O.ref_dl_minibatch(D0, Xnp, perm_np, reps, DL_BATCH, DL_LAMBDA, Ah, Bh,
+                                   1.0, 1.0 / DL_BATCH)
                 reps += 1
             rate = reps / (time.perf_counter() - t0)
             thr = omp_threads(-1)
             cpu = {"value": rate, "unit": "minibatches/s", "cores": thr, "kind": "reference",
-                   "sample": f"{reps} minibatches of {DL_BATCH} signals: reference lasso2 "
-                             f"(T=float, Gram recomputed per call), OpenMP {thr} threads; the "
-                             "A/B accumulations are not included"}
+                   "sample": f"{reps} minibatches of {DL_BATCH} signals: the reference's own "
+                             "Gram (XtX + ridge), multTrans, coreLARS2, sort and rank-1 A/B "
+                             f"accumulations (dictLearn/dicts.h:526-603, T=float), OpenMP "
+                             f"{thr} threads; D held fixed"}
         except Exception as e:
             cpu = {"value": None, "unit": "minibatches/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -731,36 +767,42 @@ def run_dictlearn(args) -> None:
     code_ms = prof["ms_code"]
     alg_bytes = 4 * DL_K * DL_BATCH + 4 * DL_K * prof["steps"] + 8 * nnz
     achieved = alg_bytes / (code_ms / 1e3) / 1e9 if code_ms > 0 else None
+    kname = "lars_cta_kernel" if prof["kernel"] == spams_b200.SC_KERNEL_CTA else "lars_kernel"
     value = done / (graph_ms / 1e3)
-    line = {
+    return {
         "metric": DL_METRIC, "value": value, "unit": "minibatches/s", "n_gpus": 1,
-        "steps": done, "warmup": args.warmup, "ms_per_step": graph_ms / done,
+        "steps": done, "warmup": warmup, "ms_per_step": graph_ms / done,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded smooth 12x12 patches, pool of 200000)",
+        "data": f"synthetic (seeded smooth 12x12 patches, pool of {pool})",
         "config": {"workload": f"dictlearn_m{DL_M}_K{DL_K}_batch{DL_BATCH}_lambda{DL_LAMBDA}",
-                   "minibatches": done, "precision": args.precision,
+                   "minibatches": done, "precision": precision,
                    "between_steps": "none (a minibatch's inputs are 0.6 MB; the loop is the unit)",
                    "launch": "one CUDA graph replay per minibatch", "parallelism": "one GPU"},
         "eager_value": ne / (eager_ms / 1e3),
         "e2e": {"value": 1.0 / e2e_s, "unit": "minibatches/s",
                 "h2d_bytes_per_step": DL_BATCH * DL_M * 4, "d2h_bytes_per_step": 8},
-        "gpu_launches": None,
-        "roofline": {"kernel": "lars_kernel", "bound": "hbm", "achieved": achieved,
+        "gpu_launches": prof["launches"] * done,
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
                      "traffic": None, "peak_source": peaks["source"],
-                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms},
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms": code_ms,
+                     "active_set_capacity": prof["lcap"]},
         "stages_ms": {k: prof[k] for k in ("ms_norms", "ms_corr", "ms_code", "ms_csc")},
         "homotopy_steps_per_signal": prof["steps"] / DL_BATCH, "nnz_per_signal": nnz / DL_BATCH,
         "clocks": clk.summary(), "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_dictlearn(args) -> None:
+    print(json.dumps(dictlearn_result(args.n or 2000, args.warmup, args.precision,
+                                      args.cpu_seconds, args.no_cpu_baseline)), flush=True)
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["lasso", "uneven_omp", "serve", "dictlearn"],
@@ -774,6 +816,11 @@ def main() -> int:
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=3, help="serve: concurrent launches")
     ap.add_argument("--no-sweep", action="store_true", help="serve: skip the lower rates")
+    ap.add_argument("--no-sub-workloads", action="store_true",
+                    help="lasso: leave the uneven-OMP, dictionary-learning and serving "
+                         "sub-objects out of the line")
+    ap.add_argument("--uneven-n", type=int, default=200000,
+                    help="signals of the uneven-OMP sub-workload of the default line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed steps
     if args.workload == "uneven_omp":

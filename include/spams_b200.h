@@ -111,6 +111,9 @@ typedef struct {
   int64_t signals;     /* signals coded */
   int64_t steps;       /* OMP / LARS steps summed over the signals (profile) */
   int64_t overflowed;  /* signals rerun with global-memory state (profile) */
+  int32_t kernel;      /* coding kernel family of the last chunk: SC_KERNEL_WARP or
+                          SC_KERNEL_CTA */
+  int32_t lcap;        /* its active-set capacity in shared memory (atoms) */
 } sc_profile;
 
 /* ---- library / status ------------------------------------------------- */
@@ -216,11 +219,13 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
  *   The caller passes inputs and output as for sc_corr_f32_dev; the hi / lo
  *   halves of D and X are staged in a fixed 16 MiB array compiled into the
  *   library (held on every GPU that loads the library until exit), so
- *   256 + 4 * m64 * (K + n) bytes must fit in 16 MiB, m64 = m rounded up to a
- *   multiple of 64 (larger calls return SC_ERR_CAPACITY; split X by columns).
+ *   256 + 2 * r(2 * m64 * K) + 2 * r(2 * m64 * n) bytes must fit in 16 MiB,
+ *   m64 = m rounded up to a multiple of 64 and r(b) = b rounded up to a
+ *   multiple of 256 (larger calls return SC_ERR_CAPACITY; split X by columns).
  *   The first call on a device looks up the array's address there (make it
  *   before any stream capture).  All calls share the array: calls that
- *   overlap on the GPU race and must be serialised.  The call returns after
+ *   overlap on the GPU race and must be serialised.  Every call synchronises
+ *   its stream (it reads back the pipeline's timeout flag) and returns after
  *   the stream has finished the product.  No cudaMalloc / cudaFree or other
  *   allocating routine is called. */
 sc_status sc_corr_bf16x3_noalloc_f32(const float* dD, int m, int K, const float* dX, int64_t n,

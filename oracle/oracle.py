@@ -167,6 +167,22 @@ def ref_lasso(X, D=None, Q=None, q=None, L=-1, lambda1=0.0, lambda2=0.0, mode=2,
     return (a, path) if return_reg_path else a
 
 
+def ref_dl_minibatch(D, X, perm, it, batch, lambda1, A, B, beta=1.0, gamma=1.0, numThreads=-1):
+    """One minibatch of the reference's online dictionary learning (coding and
+    accumulations, dictLearn/dicts.h:526-603, PENALTY mode) in float32: A and
+    B (Fortran float32 arrays K x K and m x K) are updated in place."""
+    D = _f(D, np.float32)
+    X = _f(X, np.float32)
+    perm = np.ascontiguousarray(perm, np.int32)
+    m, K = D.shape
+    assert A.dtype == np.float32 and A.flags.f_contiguous and A.shape == (K, K)
+    assert B.dtype == np.float32 and B.flags.f_contiguous and B.shape == (m, K)
+    lib = _ref_lib()
+    lib.ref_dl_minibatch_f32(_p(D), C.c_int(m), C.c_int(K), _p(X), C.c_int(X.shape[1]), _p(perm),
+                             C.c_int(it), C.c_int(batch), C.c_float(lambda1), C.c_int(numThreads),
+                             _p(A), _p(B), C.c_float(beta), C.c_float(gamma))
+
+
 # ---------------------------------------------------------------------------
 # the C restatement
 

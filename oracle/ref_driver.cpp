@@ -16,12 +16,19 @@
 //                       decomp/decomp.h:406-519)
 //   ref_lasso_mask_* -> _lassoMask<T> cpp_library/spams.h:191-214 (lasso_mask,
 //                       decomp/decomp.h:1466-1561)
+//   ref_dl_minibatch_f32 -> one minibatch of Trainer<T>::train
+//                       (dictLearn/dicts.h:526-603): XtX Gram + ridge, per
+//                       signal multTrans + coreLARS2 + sort, per-thread
+//                       rank-1 accumulations AT += a a^T, BT += x a^T, summed
+//                       into A and B (PENALTY mode, the reference's own code
+//                       called in its order; the D update is not part of it)
 // Outputs are copied out of the reference's SpMatrix<T> (linalg/linalg.h:775-935)
 // into malloc'd CSC arrays released by ref_free().
 #include "cppspams.h"
 #include <cstdlib>
 #include <cstring>
 #include <cstdint>
+#include <vector>
 
 extern "C" {
 
@@ -184,7 +191,82 @@ static int run_lasso_mask(const T* X, int m, int n, const T* D, int K, const uin
   return 0;
 }
 
+// One minibatch of the reference's online dictionary learning, coding and
+// accumulation part (dictLearn/dicts.h:526-603, PENALTY mode): the same
+// calls in the same order on the reference's own classes.  A = beta A +
+// gamma sum_j a_j a_j^T, B = beta B + gamma sum_j x_j a_j^T.
+template <typename T>
+static int run_dl_minibatch(const T* D, int m, int K, const T* X, int M, const int* perm,
+                            int iter, int batch, T lambda1, T lambda2, int numThreads, T* A,
+                            T* B, T beta, T gamma) {
+  Matrix<T> mD(const_cast<T*>(D), m, K);
+  Matrix<T> mX(const_cast<T*>(X), m, M);
+  Matrix<T> mA(A, K, K), mB(B, m, K);
+  const int L = MIN(m, K);
+  const int NT = init_omp(numThreads);
+  Matrix<T> G;
+  mD.XtX(G);
+  G.addDiag(MAX(lambda2, T(1e-10)));
+  std::vector<Matrix<T>> AT(NT), BT(NT), GsT(NT), GaT(NT), invGsT(NT), workT(NT);
+  std::vector<Vector<T>> DtRT(NT), uT(NT), XT(NT);
+  std::vector<SpVector<T>> spT(NT);
+  for (int t = 0; t < NT; ++t) {
+    AT[t].resize(K, K); AT[t].setZeros();
+    BT[t].resize(m, K); BT[t].setZeros();
+    GsT[t].resize(L, L); invGsT[t].resize(L, L); GaT[t].resize(K, L);
+    workT[t].resize(K, 3); workT[t].setZeros();
+    DtRT[t].resize(K); uT[t].resize(K); uT[t].setZeros(); XT[t].resize(m);
+    spT[t].resize(L);
+  }
+  int j;
+#pragma omp parallel for private(j)
+  for (j = 0; j < batch; ++j) {
+#ifdef _OPENMP
+    const int t = omp_get_thread_num();
+#else
+    const int t = 0;
+#endif
+    const int index = perm[((int64_t)j + (int64_t)iter * batch) % M];
+    Vector<T>& Xj = XT[t];
+    mX.copyCol(index, Xj);
+    mD.multTrans(Xj, DtRT[t]);
+    SpVector<T>& sp = spT[t];
+    sp.setL(L);
+    Vector<INTM> ind;
+    Vector<T> coeffs;
+    sp.refIndices(ind);
+    sp.refVal(coeffs);
+    T normX = Xj.nrm2sq();
+    coeffs.setZeros();
+    coreLARS2(DtRT[t], G, GsT[t], GaT[t], invGsT[t], uT[t], coeffs, ind, workT[t], normX,
+              PENALTY, lambda1, false);
+    int cnt = 0;
+    for (int k = 0; k < L; ++k) {
+      if (ind[k] == -1) break;
+      ++cnt;
+    }
+    sort(ind.rawX(), coeffs.rawX(), (INTM)0, (INTM)(cnt - 1));
+    sp.setL(cnt);
+    AT[t].rank1Update(sp);
+    BT[t].rank1Update(Xj, sp);
+  }
+  mA.scal(beta);
+  mB.scal(beta);
+  for (int t = 0; t < NT; ++t) {
+    mA.add(AT[t], gamma);
+    mB.add(BT[t], gamma);
+  }
+  return 0;
+}
+
 extern "C" {
+
+int ref_dl_minibatch_f32(const float* D, int m, int K, const float* X, int M, const int* perm,
+                         int iter, int batch, float lambda1, int numThreads, float* A, float* B,
+                         float beta, float gamma) {
+  return run_dl_minibatch<float>(D, m, K, X, M, perm, iter, batch, lambda1, 0.f, numThreads, A,
+                                 B, beta, gamma);
+}
 
 int ref_omp_mask_f64(const double* X, int m, int n, const double* D, int K, const uint8_t* B,
                      const int* L, int nL, const double* eps, int nEps, const double* lambda,

@@ -220,18 +220,25 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   const int mp = tc_pad_m(m);
   if (tc) SC_TRY(s->split.reserve((size_t)mp * K * 4));
 
+  // the thread's sc_profile describes this step: its launches always, its
+  // coding stages' times when profiling is on
+  profile_reset();
+  int own_launches = 0;
   // 1. Gram with the ridge (and the BF16 split of the updated D)
   float* G = reinterpret_cast<float*>(s->G.ptr);
   const float ridge = std::max(s->lambda2, 1e-10f);
   SC_CUDA(launch_gram<float>(dD, m, K, Kp, ridge, G, st));
+  own_launches += 2;
   if (tc) {
     char* sp = static_cast<char*>(s->split.ptr);
     SC_CUDA(launch_bf16_split(dD, m, m, K, mp, sp, sp + (size_t)mp * K * 2, st));
+    own_launches += 1;
   }
   // 2. the minibatch
   float* Xb = reinterpret_cast<float*>(s->Xb.ptr);
   dl_gather_kernel<<<n, 128, 0, st>>>(dX, m, M, dperm, d_iter, n, Xb);
   SC_CUDA(cudaGetLastError());
+  own_launches += 1;
   // 3. its codes
   BatchDesc b;
   b.lars = s->mode <= 2;
@@ -264,7 +271,6 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   b.cap = (int64_t)n * L;
   b.stream = st;
   b.profile = s->profile;
-  if (s->profile) profile_reset();
   SC_TRY(code_batch_f32(*s->ctx, b));
   // 4. A and B
   if (dA || dB) {
@@ -293,10 +299,12 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
     dl_accumulate_kernel<<<K, 256, smem, st>>>(colptr, rows, vals, Xb, m, K, ptrK, sigK, valK, dA,
                                                dB, beta, gamma);
     SC_CUDA(cudaGetLastError());
+    own_launches += 7;  // count, the three scan kernels, fill, sort, accumulate
   }
   // 5. next minibatch
   dl_advance_kernel<<<1, 1, 0, st>>>(d_iter);
   SC_CUDA(cudaGetLastError());
+  profile_add_launches(own_launches + 1);
   return SC_OK;
 }
 

@@ -229,6 +229,7 @@ struct Prof {
 
 static void prof_reset() { memset(&g_prof, 0, sizeof(g_prof)); }
 void profile_reset() { prof_reset(); }
+void profile_add_launches(int k) { g_prof.launches += k; }
 
 // Blocks of the refinement pass for active sets beyond 32 atoms.
 constexpr int kRefineBigGrid = 32;
@@ -697,6 +698,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     if (chosen < 0) SC_TRY(tune(cn, code, chosen));
     const Shape& shp = cands[(size_t)chosen];
     const bool may_overflow = shp.Lcap < p.L;
+    g_prof.kernel = shp.cta ? SC_KERNEL_CTA : SC_KERNEL_WARP;
+    g_prof.lcap = shp.Lcap;
     pr.mark(ST_CODE);
     SC_TRY(code(shp, cn, true));
     // ---- double-precision solves on the final active sets: the ols

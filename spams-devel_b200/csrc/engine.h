@@ -109,6 +109,8 @@ struct BatchDesc {
   bool profile = false;  // per-stage device times into the thread's sc_profile (synchronises)
 };
 void profile_reset();
+// Adds k engine kernel launches to the calling thread's sc_profile.
+void profile_add_launches(int k);
 sc_status code_batch_f32(DeviceCtx& c, const BatchDesc& b);
 sc_status finish_batch(DeviceCtx& c, const BatchDesc& b, int64_t* nnz);
 int pad_atoms(int K);

@@ -23,6 +23,7 @@
 #include "kernels.h"
 #include "refactor.cuh"
 #include "masked.cuh"
+#include "lars_screen.cuh"
 
 namespace sc {
 
@@ -308,59 +309,12 @@ lars_kernel(const LarsArgs<T> a) {
           }
         }
 
-        // ---- joining steps: first minimum magnitude over the 2K candidates.
-        // Row r offers (C + c_r)/(1 + a_r) (index r) and (C - c_r)/(1 - a_r)
-        // (index r + K); with both denominators positive the first is the
-        // smaller one exactly when c_r <= C a_r (ties go to index r), so each
-        // row submits one candidate, or its other one when the first has no
-        // positive denominator (pos submits only the second).  Candidates
-        // are fractions num/den, den > 0, compared by cross-multiplication in
-        // four independent chains (one per row offset e); each lane's winner
-        // is divided exactly and the warp reduces the exact (|value|, index)
-        // pairs, ties to the first index as in cblas_iamin.  Infinite
-        // candidates (active or padding atoms, |A_j| beyond the bounds) never
-        // decide a step (the step is then step_max or step_max2).
-        T cn[4], cd[4];
-        int ci[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) { cn[e] = INF; cd[e] = T(1); ci[e] = 0x7fffffff; }
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const int r0 = v * 128 + lane * 4;
-          const Vec4<T> d = ld4(sDtR + r0);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int r = r0 + e;
-            const bool active = (act >> (v * 4 + e)) & 1u;  // padding rows are marked active
-            const T aa = A[v][e], c = d.v[e];
-            const bool okp = !pos && aa > T(-1) && aa < INF;  // (C + c)/(1 + a) admissible
-            const bool okm = aa < T(1);                       // (C - c)/(1 - a) admissible
-            const bool plus = okp && (!okm || c <= C * aa);
-            const T num = plus ? C + c : C - c;
-            const T den = plus ? T(1) + aa : T(1) - aa;
-            const int idx = plus ? r : r + K;
-            const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
-            const bool take = !active && (okp || okm) && (lhs < rhs || (lhs == rhs && idx < ci[e]));
-            cn[e] = take ? num : cn[e];
-            cd[e] = take ? den : cd[e];
-            ci[e] = take ? idx : ci[e];
-          }
-        }
-#pragma unroll
-        for (int h = 1; h < 4; h <<= 1) {
-#pragma unroll
-          for (int e = 0; e + h < 4; e += 2 * h) {
-            const T lhs = fabs(cn[e + h]) * cd[e], rhs = fabs(cn[e]) * cd[e + h];
-            if (lhs < rhs || (lhs == rhs && ci[e + h] < ci[e])) {
-              cn[e] = cn[e + h]; cd[e] = cd[e + h]; ci[e] = ci[e + h];
-            }
-          }
-        }
-        int midx = ci[0];
-        T mval = cn[0] / cd[0];
-        T mkey = fabs(mval);
-        if (!(mkey < INF)) { mkey = INF; mval = INF; }  // NaN never wins
-        const ArgRes<T> mr = warp_argmin_first(mkey, midx, mval);  // warp-uniform
+        // ---- joining steps: first minimum magnitude over the 2K candidates
+        // (lars_screen.cuh); infinite candidates (active or padding atoms,
+        // |A_j| beyond the bounds) never decide a step (the step is then
+        // step_max or step_max2)
+        const ScreenBest<T> sb = lars_screen<NV>(A, sDtR + lane * 4, lane * 4, act, C, pos, K);
+        const ArgRes<T> mr = warp_argmin_first(sb.key, sb.idx, sb.val);  // warp-uniform
         T step = mr.val;
         cur = mr.idx % K;
 

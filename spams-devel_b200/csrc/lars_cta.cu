@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "refactor.cuh"
+#include "lars_screen.cuh"
 
 namespace sc {
 
@@ -244,48 +245,11 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
 #pragma unroll
           for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
         }
-        // ---- joining candidates (one per row, as in the warp kernel)
-        T cn[4], cd[4];
-        int ci[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) { cn[e] = INF; cd[e] = T(1); ci[e] = 0x7fffffff; }
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const int r0 = rbase + v * 128 + lane * 4;
-          const Vec4<T> d = ld4(sDtR + r0);
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int r = r0 + e;
-            const bool active = (act >> (v * 4 + e)) & 1u;
-            const T aa = A[v][e], c = d.v[e];
-            const bool okp = !pos && aa > T(-1) && aa < INF;
-            const bool okm = aa < T(1);
-            const bool plus = okp && (!okm || c <= C * aa);
-            const T num = plus ? C + c : C - c;
-            const T den = plus ? T(1) + aa : T(1) - aa;
-            const int idx = plus ? r : r + K;
-            const T lhs = fabs(num) * cd[e], rhs = fabs(cn[e]) * den;
-            const bool take = !active && (okp || okm) && (lhs < rhs || (lhs == rhs && idx < ci[e]));
-            cn[e] = take ? num : cn[e];
-            cd[e] = take ? den : cd[e];
-            ci[e] = take ? idx : ci[e];
-          }
-        }
-#pragma unroll
-        for (int h = 1; h < 4; h <<= 1) {
-#pragma unroll
-          for (int e = 0; e + h < 4; e += 2 * h) {
-            const T lhs = fabs(cn[e + h]) * cd[e], rhs = fabs(cn[e]) * cd[e + h];
-            if (lhs < rhs || (lhs == rhs && ci[e + h] < ci[e])) {
-              cn[e] = cn[e + h]; cd[e] = cd[e + h]; ci[e] = ci[e + h];
-            }
-          }
-        }
+        // ---- joining candidates of the own rows (lars_screen.cuh)
         {
-          T mval = cn[0] / cd[0];
-          T mkey = fabs(mval);
-          if (!(mkey < INF)) { mkey = INF; mval = INF; }
-          const ArgRes<T> mr = warp_argmin_first(mkey, ci[0], mval);
+          const ScreenBest<T> sb =
+              lars_screen<NV>(A, sDtR + rbase + lane * 4, rbase + lane * 4, act, C, pos, K);
+          const ArgRes<T> mr = warp_argmin_first(sb.key, sb.idx, sb.val);
           if (lane == 0) { exK[gw] = fabs(mr.val) < INF ? fabs(mr.val) : INF; exV[gw] = mr.val; exI[gw] = mr.idx; }
         }
         __syncthreads();

@@ -13,7 +13,8 @@ device.  `Server` keeps dictionaries resident and codes a stream of requests
 `MinibatchStep` is the graph-capturable minibatch step of online dictionary
 learning.
 """
-from ._lib import (SC_L1COEFFS, SC_L2ERROR, SC_PENALTY, SC_PREC_BF16X3, SC_PREC_FP32,  # noqa: F401
+from ._lib import (SC_KERNEL_AUTO, SC_KERNEL_CTA, SC_KERNEL_WARP,  # noqa: F401
+                   SC_L1COEFFS, SC_L2ERROR, SC_PENALTY, SC_PREC_BF16X3, SC_PREC_FP32,
                    ScError, device_count, last_error, last_profile, lib)
 from .api import (corr_device, lasso, lasso_device, lassoMask, omp, omp_device,  # noqa: F401
                   ompMask)

@@ -67,7 +67,7 @@ class Profile(C.Structure):
                 ("ms_code", C.c_double), ("ms_refine", C.c_double), ("ms_csc", C.c_double),
                 ("ms_total", C.c_double),
                 ("launches", C.c_int64), ("signals", C.c_int64), ("steps", C.c_int64),
-                ("overflowed", C.c_int64)]
+                ("overflowed", C.c_int64), ("kernel", C.c_int32), ("lcap", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -102,6 +102,26 @@ def rel_err(a, b):
     return float(nd / nb) if nb > 0 else float(nd)
 
 
+def col_rel_errs(a, b):
+    """Per-column relative errors ||a_j - b_j|| / ||b_j|| (0 where both are
+    empty), in float64."""
+    a = a.tocsc().astype(np.float64)
+    b = b.tocsc().astype(np.float64)
+    d = a - b
+    nd = np.sqrt(np.asarray(d.power(2).sum(axis=0)).ravel())
+    nb = np.sqrt(np.asarray(b.power(2).sum(axis=0)).ravel())
+    return np.where(nb > 0, nd / np.where(nb > 0, nb, 1.0), nd)
+
+
+def err_report(a, b):
+    """(support match, Frobenius rel err, 99.9th-percentile and max per-column
+    rel err over the columns whose supports agree)."""
+    sm = support_match(a, b)
+    am, bm = matched_columns(a, b)
+    ce = col_rel_errs(am, bm) if am.shape[1] else np.zeros(1)
+    return sm, rel_err(am, bm), float(np.percentile(ce, 99.9)), float(ce.max())
+
+
 @pytest.fixture(scope="session")
 def gpu_available():
     import spams_b200

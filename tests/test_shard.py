@@ -1,8 +1,9 @@
-"""Multi-GPU column sharding, exercised on CPU with two gloo ranks.
+"""Multi-GPU column sharding with two gloo ranks.
 
-Each rank codes its column block with the CPU oracle standing in for its GPU
-(the sharding logic is the same); the gathered result must equal the
-unsharded coding of the whole batch."""
+On the CPU each rank codes its column block with the oracle standing in for
+its GPU; on a GPU box both ranks code with the engine itself on the one GPU.
+Either way the blocks travel as flat CSC arrays and the gathered result must
+equal the unsharded coding of the whole batch."""
 import os
 import socket
 
@@ -87,3 +88,52 @@ def test_two_gloo_ranks_code_like_one():
     assert abs(gathered[0] - ref).max() == 0
     for r in res:  # all ranks hold the all-gathered OMP result
         assert abs(r[2] - refo).max() == 0
+
+
+def _gpu_worker(rank, world, port, q):
+    """Two ranks on one GPU coding their blocks with the engine itself (the
+    ranks never wait on each other inside a kernel)."""
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import spams_b200
+        from spams_b200 import workloads as W
+        from spams_b200.shard import code_sharded
+        X, D = W.config_lasso(n=3001, seed=9, m=64, K=256, s=6, noise=0.01)
+        a = code_sharded(spams_b200.lasso, X.astype(np.float32), D.astype(np.float32),
+                         lambda1=0.1)
+        Xo, Do, Lv, ev = W.config_uneven_omp(n=1577, seed=10, m=48, K=128, smax=12)
+        b = code_sharded(spams_b200.omp, Xo, Do, L=Lv, eps=ev, dst=None)
+        q.put(("ok", a, b))
+    except Exception as e:
+        q.put(("err", repr(e), None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_two_gloo_ranks_with_the_engine_code_like_one():
+    import multiprocessing as mp
+    import spams_b200
+    from spams_b200 import workloads as W
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(r[0] == "ok" for r in res), res
+    X, D = W.config_lasso(n=3001, seed=9, m=64, K=256, s=6, noise=0.01)
+    ref = spams_b200.lasso(X.astype(np.float32), D.astype(np.float32), lambda1=0.1)
+    Xo, Do, Lv, ev = W.config_uneven_omp(n=1577, seed=10, m=48, K=128, smax=12)
+    refo = spams_b200.omp(Xo, Do, L=Lv, eps=ev)
+    gathered = [r[1] for r in res if r[1] is not None]
+    assert len(gathered) == 1
+    assert abs(gathered[0] - ref).max() == 0 and gathered[0].nnz == ref.nnz
+    for r in res:
+        assert abs(r[2] - refo).max() == 0 and r[2].nnz == refo.nnz
