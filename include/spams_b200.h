@@ -83,10 +83,12 @@ typedef struct {
   int kernel;     /* SC_KERNEL_*: which coding kernels may run; default
                      SC_KERNEL_AUTO (timed once per shape, then cached).
                      Every choice gives the same results. */
-  int refactor;   /* single-precision Lasso: 0 (default) rebuilds the active
-                     set's inverse Gram in FP64 when an added atom's pivot
-                     falls below 1e-3 of its diagonal (active sets up to 32
-                     atoms); > 0 on every added atom; < 0 never */
+  int refactor;   /* single-precision calls: 0 (default) rebuilds the active
+                     set's state in FP64 when an added atom's pivot falls
+                     below 1e-3 of its diagonal (Lasso: the inverse Gram;
+                     OMP: the inverse Cholesky factor, the projections RUn and
+                     the residual norm), for active sets up to 96 atoms;
+                     > 0 on every added atom; < 0 never */
   int reserved[2];
 } sc_options;
 

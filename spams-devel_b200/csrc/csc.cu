@@ -3,6 +3,10 @@
 // coefficient) pairs already sorted by atom index in an n x L slab; here the
 // sizes are scanned into column pointers and the pairs are gathered into the
 // contiguous row / value arrays, one warp per column.
+//
+// Also here: the longest-first order of a persistent launch over signals with
+// per-signal step caps L_i (a counting sort by descending L_i), so that the
+// signals with the most steps start first and the shortest ones fill the tail.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -135,6 +139,75 @@ cudaError_t launch_csc_gather(const int* slab_ind, const T* slab_val, int L, con
   if (n <= 0) return cudaSuccess;
   csc_gather_kernel<T><<<(unsigned)((n + 7) / 8), 256, 0, st>>>(
       slab_ind, slab_val, L, cnt, colptr, n, sub, cap, capflag, rows, vals);
+  return cudaGetLastError();
+}
+
+// ---- longest-first order: bin k holds the signals with min(L_i, Lmax) = Lmax - k
+__device__ __forceinline__ int order_bin(const int* vL, int64_t i, int Lmax) {
+  const int l = vL[i];
+  return Lmax - (l < 0 ? 0 : (l > Lmax ? Lmax : l));
+}
+
+__global__ void order_hist_kernel(const int* vL, int64_t n, int Lmax, int* hist) {
+  extern __shared__ int sh[];
+  const int nb = Lmax + 1;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) sh[b] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&sh[order_bin(vL, i, Lmax)], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    if (sh[b]) atomicAdd(&hist[b], sh[b]);
+}
+
+// Exclusive scan of the nb bin counts in place (one block).
+__global__ void order_scan_kernel(int* hist, int nb) {
+  if (threadIdx.x != 0) return;
+  int run = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int v = hist[b];
+    hist[b] = run;
+    run += v;
+  }
+}
+
+// Tiles of blockDim signals: each tile reserves its range of every bin with
+// one global atomic per bin, then places its signals in it.
+__global__ void order_scatter_kernel(const int* vL, int64_t n, int Lmax, int* offs,
+                                     int64_t* list) {
+  extern __shared__ int sh[];
+  const int nb = Lmax + 1;
+  int* scnt = sh;
+  int* sbase = sh + nb;
+  for (int64_t t0 = (int64_t)blockIdx.x * blockDim.x; t0 < n; t0 += (int64_t)gridDim.x * blockDim.x) {
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) scnt[b] = 0;
+    __syncthreads();
+    const int64_t i = t0 + threadIdx.x;
+    const int b = i < n ? order_bin(vL, i, Lmax) : 0;
+    const int local = i < n ? atomicAdd(&scnt[b], 1) : 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+      if (scnt[k]) sbase[k] = atomicAdd(&offs[k], scnt[k]);
+    __syncthreads();
+    if (i < n) list[sbase[b] + local] = i;
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_order_by_L_desc(const int* vL, int64_t n, int Lmax, int* scratch,
+                                   int64_t* list, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  if (Lmax < 0 || Lmax > kOrderMaxL) return cudaErrorInvalidValue;
+  const int nb = Lmax + 1;
+  cudaError_t e = cudaMemsetAsync(scratch, 0, (size_t)nb * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (n + 255) / 256;
+  const unsigned blocks = (unsigned)(tiles < 148 * 8 ? tiles : 148 * 8);
+  order_hist_kernel<<<blocks, 256, (size_t)nb * sizeof(int), st>>>(vL, n, Lmax, scratch);
+  order_scan_kernel<<<1, 32, 0, st>>>(scratch, nb);
+  order_scatter_kernel<<<blocks, 256, (size_t)2 * nb * sizeof(int), st>>>(vL, n, Lmax, scratch,
+                                                                          list);
   return cudaGetLastError();
 }
 

@@ -305,7 +305,7 @@ struct Problem {
   bool refine = false;            // FP64 refinement of the final coefficients
   bool ols = false;               // least-squares refit on the final support (lasso ols)
   int kernel = SC_KERNEL_AUTO;    // SC_KERNEL_*: kernel family (AUTO: tuned)
-  int refactor = 1;               // LARS FP64 refactor: 0 never, 1 small pivots, 2 always
+  int refactor = 1;               // FP64 refactor: 0 never, 1 small pivots, 2 always
   // masked variants (lasso_mask / omp_mask): host row mask m x n, the ridge of
   // the masked Grams, and whether the Lasso constraint is scaled by the
   // observed fraction (PENALTY / L2ERROR; OMP always scales eps)
@@ -370,12 +370,14 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
   std::vector<Shape> cands = candidates_for<T>(c, p.lars, Kp, p.L, p.kernel);
-  // FP64 refactor of single-precision LARS: one 16 KB scratch per warp (warp
-  // kernels) or CTA (CTA kernels, whose grid is then fixed here)
-  const bool refac = p.lars && sizeof(T) == 4 && p.refactor != 0;
+  // FP64 refactor of the single-precision state (refactor.cuh): one scratch
+  // unit per warp (warp kernels) or CTA (CTA kernels, whose grid is then fixed
+  // here)
+  const bool refac = sizeof(T) == 4 && p.refactor != 0;
   if (refac)
     for (Shape& sh : cands)
-      if (sh.cta) sh.grid = lars_cta_grid<T>(Kp, sh.Lcap, false);
+      if (sh.cta)
+        sh.grid = p.lars ? lars_cta_grid<T>(Kp, sh.Lcap, false) : omp_cta_grid<T>(Kp, sh.Lcap, false);
   const bool piped = sink && p.hX && !p.hmask;
   const int nbuf = piped ? 2 : 1;
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
@@ -402,6 +404,12 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   }
   if (p.tc) SC_TRY(c.xsplit.reserve((size_t)nc * p.mp * 4));
   SC_TRY(c.level.reserve((size_t)nc * sizeof(T)));
+  // OMP with per-signal step caps: each launch takes its signals longest first
+  const bool ordered = !p.lars && p.dLv && p.L <= kOrderMaxL;
+  if (ordered) {
+    SC_TRY(c.order.reserve((size_t)nc * 8));
+    SC_TRY(c.ordscr.reserve((size_t)(p.L + 1) * 4));
+  }
   const size_t col_slot = align16((size_t)(nc + 1) * 8);
   const size_t ent_slot = (size_t)nc * p.L;
   if (sink) {
@@ -427,15 +435,20 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   };
   for (const Shape& sh : cands)
     if (sh.Lcap < p.L) SC_TRY(c.gstate.reserve(ovf_plan(sh).bytes));
-  const size_t rf_unit = (size_t)2 * kRefactorMax * kRefactorMax * sizeof(double);
+  // refactor scratch: the largest launch's units, each for the largest
+  // refactored active set of any launch
+  int rf_units = 0;
   if (refac) {
     size_t units = 0;
+    int cap = refactor_cap(p.L);
     for (const Shape& sh : cands) {
       units = std::max(units, (size_t)sh.grid * (sh.cta ? 1 : sh.wpb));
       const Ovf ov = ovf_plan(sh);
       units = std::max(units, (size_t)ov.grid * ov.wpb);
+      cap = std::max(cap, refactor_cap(sh.Lcap));
     }
-    SC_TRY(c.rfscr.reserve(units * rf_unit));
+    SC_TRY(c.rfscr.reserve(units * (size_t)cap * cap * sizeof(double)));
+    rf_units = (int)units;
   }
   // masked variants: Dᵀ, the chunk's mask / classes / scaled parameters, and
   // one m-vector of scratch per warp of the largest launch
@@ -634,6 +647,13 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       pr.launches(2);
     }
     // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
+    const int64_t* order = nullptr;
+    if (ordered) {
+      SC_CUDA(launch_order_by_L_desc(p.dLv + start, cn, p.L, reinterpret_cast<int*>(c.ordscr.ptr),
+                                     reinterpret_cast<int64_t*>(c.order.ptr), st));
+      pr.launches(3);
+      order = reinterpret_cast<const int64_t*>(c.order.ptr);
+    }
     int* cnt = reinterpret_cast<int*>(c.cnt.ptr);
     int* sind = reinterpret_cast<int*>(c.slab_ind.ptr);
     T* sval = reinterpret_cast<T*>(c.slab_val.ptr);
@@ -657,6 +677,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
         a.refactor = refac ? p.refactor : 0;
         a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
+        a.rf_cap = refactor_cap(shp.Lcap);
+        a.rf_units = refac ? rf_units : 0;
         if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
         else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
         if (final_run) pr.launches(1);
@@ -665,6 +687,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
           a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          a.rf_cap = refactor_cap(p.L);
           if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
           else SC_CUDA(launch_lars<T>(a, ov.grid, ov.wpb, st));
         }
@@ -676,11 +699,15 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.vEps = mvec ? mvec : (p.dEps ? p.dEps + start : nullptr);
         a.vLambda = p.dLam ? p.dLam + start : nullptr;
         a.mk = mk;
-        a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr; a.sig_list = nullptr;
+        a.n_jobs = (int)jobs; a.n_jobs_dev = nullptr; a.sig_list = order;
         a.work_counter = d_counter; a.out_ind = sind; a.out_val = sval; a.out_cnt = cnt;
         a.overflow_list = ovf_list; a.overflow_count = d_ovf_count; a.gstate = nullptr;
         a.path = final_run ? path : nullptr;
         a.steps = final_run ? d_steps : nullptr;
+        a.refactor = refac ? p.refactor : 0;
+        a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
+        a.rf_cap = refactor_cap(shp.Lcap);
+        a.rf_units = refac ? rf_units : 0;
         if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, shp.grid, st));
         else SC_CUDA(launch_omp<T>(a, shp.grid, shp.wpb, st));
         if (final_run) pr.launches(1);
@@ -689,6 +716,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
           a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          a.rf_cap = refactor_cap(p.L);
           if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, ov.grid, st));
           else SC_CUDA(launch_omp<T>(a, ov.grid, ov.wpb, st));
         }
@@ -825,14 +853,24 @@ static sc_status check_kernel(int K, const sc_options* opt) {
 
 // Per-call device guard: serialises calls on one device and orders this
 // call's stream after the previous user of the shared workspaces.
+// Orders the calls on one device's shared workspaces: a call waits for the
+// previous call's device work and marks its own end.  A call made while its
+// stream is being captured into a CUDA graph does neither (the graph's own
+// order applies; replays of a graph that uses these workspaces must not
+// overlap other calls on the device).
 struct CallGuard {
   DeviceCtx* c;
   cudaStream_t st;
   std::lock_guard<std::mutex> lk;
+  bool capturing = false;
   CallGuard(DeviceCtx* ctx, cudaStream_t s) : c(ctx), st(s), lk(ctx->mu) {
-    cudaStreamWaitEvent(st, c->last_use, 0);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    capturing = cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+    if (!capturing) cudaStreamWaitEvent(st, c->last_use, 0);
   }
-  ~CallGuard() { cudaEventRecord(c->last_use, st); }
+  ~CallGuard() {
+    if (!capturing) cudaEventRecord(c->last_use, st);
+  }
 };
 
 // Single-precision calls take SC_PREC_FP32 or SC_PREC_BF16X3; double

@@ -61,11 +61,12 @@ struct DeviceCtx {
   Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
   Buf mask, mflag, mvec, Dt, mwork;  // masked variants
   Buf rfscr;                         // FP64 refactor scratch of the LARS kernels
+  Buf order, ordscr;                 // longest-first signal order of a launch
   std::vector<Buf*> all_bufs() {
     return {&X, &D, &G, &dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc,
             &scan, &gstate, &ccolptr, &crows, &cvals, &path, &vecs, &xstage, &xsplit,
             &dsplit, &level, &rlist, &rscratch, &mask, &mflag, &mvec, &Dt, &mwork,
-            &rfscr};
+            &rfscr, &order, &ordscr};
   }
 };
 

@@ -72,10 +72,12 @@ struct LarsArgs {
   MaskArgs<T> mk;      // masked variant (mk.mask set), warp kernels only
   // FP64 refactor of the single-precision inverse Gram (refactor.cuh):
   // 0 never, 1 when an added atom's relative pivot falls below
-  // kRefactorPivot, 2 on every added atom; rf_scratch: 2 x 32 x 32 doubles per
-  // warp (warp kernels) or per CTA (CTA kernels) of the launch
+  // kRefactorPivot, 2 on every added atom; rf_scratch: rf_units units of
+  // rf_cap x rf_cap doubles, one per warp (warp kernels) or per CTA (CTA
+  // kernels) of the launch; active sets of up to rf_cap atoms are refactored
   int refactor;
   double* rf_scratch;
+  int rf_cap, rf_units;
 };
 
 template <typename T>
@@ -104,6 +106,12 @@ struct OmpArgs {
   T* path;             // K x L for signal 0, or NULL
   unsigned long long* steps;  // if set: total OMP steps are added here
   MaskArgs<T> mk;      // masked variant (mk.mask set), warp kernels only
+  // FP64 refactor of the single-precision inverse Cholesky factor when the
+  // selected atom's residual norm (its pivot) falls below kRefactorPivot (1)
+  // or on every selected atom (2); scratch as in LarsArgs
+  int refactor;
+  double* rf_scratch;
+  int rf_cap, rf_units;
 };
 
 template <typename T>
@@ -132,6 +140,9 @@ template <typename T>
 size_t omp_cta_smem_bytes(int Kp, int Lc, bool gstate);
 template <typename T>
 size_t omp_cta_gstate_bytes(int Lc, int grid);
+// The persistent grid the OMP CTA launcher fills the device with (0 on error).
+template <typename T>
+int omp_cta_grid(int Kp, int Lc, bool gstate);
 template <typename T>
 int omp_max_warps_per_sm(int Kp);
 
@@ -193,6 +204,14 @@ cudaError_t launch_csc_gather(const int* slab_ind, const T* slab_val, int L,
                               const int* cnt, const int64_t* colptr, int64_t n,
                               const int64_t* sub, int64_t cap, int* capflag,
                               int32_t* rows, T* vals, cudaStream_t st);
+
+// list[0..n) = 0..n-1 ordered by descending min(vL[i], Lmax) (ties in no
+// particular order): the longest-first schedule of a persistent launch.
+// scratch: Lmax + 1 ints; Lmax <= kOrderMaxL.  Four launches (a memset and
+// three kernels).
+constexpr int kOrderMaxL = 4096;
+cudaError_t launch_order_by_L_desc(const int* vL, int64_t n, int Lmax, int* scratch,
+                                   int64_t* list, cudaStream_t st);
 
 // ---- BF16 hi/lo split tensor-core products (sm_100a tcgen05) --------------
 bool tc_gemm_available();

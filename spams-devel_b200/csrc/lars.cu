@@ -245,11 +245,11 @@ lars_kernel(const LarsArgs<T> a) {
             const T piv = sG[i] - dot;
             // a small pivot loses digits in the update: rebuild the inverse in FP64
             bool refactored = false;
-            if (sizeof(T) == 4 && a.refactor && i < kRefactorMax && !partial &&
+            const int unit = blockIdx.x * wpb + wib;
+            if (sizeof(T) == 4 && a.refactor && i < a.rf_cap && unit < a.rf_units && !partial &&
                 (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
-              double* rs = a.rf_scratch + (size_t)(blockIdx.x * wpb + wib) * (2 * kRefactorMax * kRefactorMax);
-              refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs,
-                                               rs + kRefactorMax * kRefactorMax);
+              double* rs = a.rf_scratch + (size_t)unit * a.rf_cap * a.rf_cap;
+              refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs);
             }
             const T schur = T(1) / piv;
             if (!refactored) lane_loop<SMALL>(i, [&](int r) {

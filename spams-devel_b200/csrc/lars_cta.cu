@@ -183,11 +183,10 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
               const T piv = sG[i] - dot;
               // a small pivot loses digits in the update: rebuild the inverse in FP64
               bool refactored = false;
-              if (sizeof(T) == 4 && a.refactor && i < kRefactorMax && !false &&
+              if (sizeof(T) == 4 && a.refactor && i < a.rf_cap && (int)blockIdx.x < a.rf_units &&
                   (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
-                double* rs = a.rf_scratch + (size_t)blockIdx.x * (2 * kRefactorMax * kRefactorMax);
-                refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs,
-                                                 rs + kRefactorMax * kRefactorMax);
+                double* rs = a.rf_scratch + (size_t)blockIdx.x * a.rf_cap * a.rf_cap;
+                refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs);
               }
               const T schur = T(1) / piv;
               if (!refactored) for (int r = lane; r < i; r += 32) {

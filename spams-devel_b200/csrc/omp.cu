@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "masked.cuh"
+#include "refactor.cuh"
 
 namespace sc {
 
@@ -98,12 +99,32 @@ omp_kernel(const OmpArgs<T> a) {
         const T nc = sNorm[c];
         if (nc < 1e-8) break;
         const T invNorm = T(1) / sqrt(nc);
-        const T RU = sRdn[c] * invNorm;
+        T RU = sRdn[c] * invNorm;
+        // a small pivot (the atom's residual norm) loses digits in the
+        // single-precision factor: rebuild Un, RUn and ||r||^2 in FP64
+        bool refactored = false;
+        const int unit = blockIdx.x * wpb + wib;
+        if (sizeof(T) == 4 && a.refactor && j < a.rf_cap && unit < a.rf_units && !partial &&
+            (a.refactor == 2 || !(nc > T(kRefactorPivot)))) {
+          if (lane == 0) sInd[j] = c;
+          __syncwarp();
+          const double nx = refactor_un<T>(a.G, Kp, sInd, j + 1, a.DtX + (size_t)sig * Kp,
+                                           a.norms[sig], sUn, ldu, sRUn,
+                                           a.rf_scratch + (size_t)unit * a.rf_cap * a.rf_cap);
+          if (nx == nx) {
+            refactored = true;
+            RU = sRUn[j];
+            normX = (T)nx + RU * RU;  // the delta of this atom comes off below
+          }
+        }
         const T delta = RU * RU;
         if (delta < 2 * lambda) break;
         normX -= delta;
         if (lane == 0) { sRUn[j] = RU; sInd[j] = c; }
         if (lane == ((c & 127) >> 2)) act |= 1u << (((c >> 7) << 2) | (c & 3));
+        if (refactored) {
+          __syncwarp();
+        } else {
         // g_l = G(c, ind_l), l < j
         if (partial) {
           for (int l = 0; l < j; ++l) {
@@ -131,6 +152,7 @@ omp_kernel(const OmpArgs<T> a) {
         }
         if (lane == 0) sUn[(size_t)j * ldu + j] = T(-1) * (-invNorm);
         __syncwarp();
+        }
         if (j == L - 1 || normX <= eps) { ++j; break; }
         if (path) {
           // path(:, j) = Un_{j+1} RUn(0:j+1) scattered to the selected atoms

@@ -9,6 +9,7 @@
 // the first index of the largest score.  Used for Kp = 512 .. 4096.
 #include "common.cuh"
 #include "kernels.h"
+#include "refactor.cuh"
 
 namespace sc {
 
@@ -111,12 +112,38 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
         const T nc = sNorm[c];
         if (nc < 1e-8) break;
         const T invNorm = T(1) / sqrt(nc);
-        const T RU = sRdn[c] * invNorm;
+        T RU = sRdn[c] * invNorm;
+        // a small pivot (the atom's residual norm) loses digits in the
+        // single-precision factor: warp 0 rebuilds Un, RUn and ||r||^2 in FP64
+        // (the decision is the same in every warp: nc comes from shared memory)
+        bool refactored = false;
+        if (sizeof(T) == 4 && a.refactor && j < a.rf_cap && (int)blockIdx.x < a.rf_units &&
+            (a.refactor == 2 || !(nc > T(kRefactorPivot)))) {
+          if (gw == 0) {
+            if (lane == 0) sInd[j] = c;
+            __syncwarp();
+            const double nx = refactor_un<T>(a.G, Kp, sInd, j + 1, a.DtX + (size_t)sig * Kp,
+                                             a.norms[sig], sUn, ldu, sRUn,
+                                             a.rf_scratch + (size_t)blockIdx.x * a.rf_cap * a.rf_cap);
+            if (lane == 0) exK[0] = (T)nx;
+          }
+          __syncthreads();
+          const T nx = exK[0];
+          __syncthreads();  // exK is reused by the next exchange
+          if (nx == nx) {
+            refactored = true;
+            RU = sRUn[j];
+            normX = nx + RU * RU;  // the delta of this atom comes off below
+          }
+        }
         const T delta = RU * RU;
         if (delta < 2 * lambda) break;
         normX -= delta;
         if (gw == own_w(c) && lane == own_l(c)) act |= 1u << own_b(c);
-        if (gw == 0) {
+        if (gw == 0 && refactored) {
+          if (lane == 0) { sRUn[j] = RU; sInd[j] = c; }
+          __syncwarp();
+        } else if (gw == 0) {
           if (lane == 0) { sRUn[j] = RU; sInd[j] = c; }
           const T* gcol = a.G + (size_t)c * Kp;
           for (int l = lane; l < j; l += 32) sGg[l] = gcol[sInd[l]];
@@ -260,6 +287,32 @@ static cudaError_t launch_w(const OmpArgs<T>& a, int grid, size_t smem, cudaStre
   return cudaGetLastError();
 }
 
+template <typename T, int W>
+static int grid_w(size_t smem) {
+  auto k = omp_cta_kernel<T, W>;
+  if constexpr (sizeof(T) == 4) k = more_resident(k, omp_cta_kernel_lb<T, W>, W * 32, smem);
+  int grid = 0;
+  if (allow_smem(k, smem) != cudaSuccess || fill_grid(k, W * 32, smem, &grid) != cudaSuccess)
+    return 0;
+  return grid;
+}
+
+template <typename T>
+int omp_cta_grid(int Kp, int Lc, bool gstate) {
+  const size_t smem = omp_cta_smem(Kp, Lc, sizeof(T), Kp / 512, gstate);
+  switch (Kp / 512) {
+    case 1: return grid_w<T, 1>(smem);
+    case 2: return grid_w<T, 2>(smem);
+    case 3: return grid_w<T, 3>(smem);
+    case 4: return grid_w<T, 4>(smem);
+    case 5: return grid_w<T, 5>(smem);
+    case 6: return grid_w<T, 6>(smem);
+    case 7: return grid_w<T, 7>(smem);
+    case 8: return grid_w<T, 8>(smem);
+    default: return 0;
+  }
+}
+
 template <typename T>
 size_t omp_cta_smem_bytes(int Kp, int Lc, bool gstate) {
   return omp_cta_smem(Kp, Lc, sizeof(T), Kp / 512, gstate);
@@ -288,6 +341,8 @@ cudaError_t launch_omp_cta(const OmpArgs<T>& a, int grid, cudaStream_t st) {
 
 template size_t omp_cta_smem_bytes<float>(int, int, bool);
 template size_t omp_cta_smem_bytes<double>(int, int, bool);
+template int omp_cta_grid<float>(int, int, bool);
+template int omp_cta_grid<double>(int, int, bool);
 template size_t omp_cta_gstate_bytes<float>(int, int);
 template size_t omp_cta_gstate_bytes<double>(int, int);
 template cudaError_t launch_omp_cta<float>(const OmpArgs<float>&, int, cudaStream_t);

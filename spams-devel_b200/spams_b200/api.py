@@ -122,7 +122,7 @@ def _vec(v, dtype, n: int):
 
 
 def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=-1,
-        precision=None, device=0, refine=None, kernel=None):
+        precision=None, device=0, refine=None, kernel=None, refactor=None):
     """Orthogonal Matching Pursuit of every column of X on D (unit-norm atoms).
 
     Mirrors spams.omp (swig/python/spams.py:167-198): L / eps / lambda1 are
@@ -144,7 +144,7 @@ def omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=
     out = CscF64() if f64 else CscF32()
     ct = C.c_double if f64 else C.c_float
     fn = _lib.lib().sc_omp_f64 if f64 else _lib.lib().sc_omp_f32
-    o = _opts(precision, device, refine=refine, kernel=kernel)
+    o = _opts(precision, device, refine=refine, kernel=kernel, refactor=refactor)
     st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Lv, C.c_int32), nL, _ptr(ev, ct), nE,
             _ptr(lv, ct), nLa, numThreads, _ptr(path, ct), C.byref(o), C.byref(out))
     _raise(st)

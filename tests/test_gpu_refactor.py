@@ -1,4 +1,5 @@
-"""FP64 refactor of the single-precision LARS inverse Gram.
+"""FP64 refactor of the single-precision active-set state: the LARS inverse
+Gram, and the OMP inverse Cholesky factor with its projections.
 
 By default it only triggers when an added atom's pivot falls below 1e-3 of
 its diagonal, which well-conditioned dictionaries never reach (the codes are
@@ -48,3 +49,60 @@ def test_refactor_on_every_add_tracks_the_fp64_path_on_near_duplicate_atoms():
     # the warp and CTA kernels refactor alike
     _same(spams_b200.lasso(Xf, Df, lambda1=0.02, refactor="always", kernel="warp"),
           spams_b200.lasso(Xf, Df, lambda1=0.02, refactor="always", kernel="cta"))
+
+
+def _near_duplicates(seed, m=64, K0=150, ndup=50, scale=1e-2):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    D0 = W.gaussian_dictionary(m, K0, rng)
+    dup = D0[:, :ndup] + scale * rng.standard_normal((m, ndup))
+    D = np.hstack([D0, dup])
+    return np.asfortranarray(D / np.linalg.norm(D, axis=0, keepdims=True)), rng
+
+
+def test_omp_default_refactor_leaves_well_conditioned_codes_unchanged():
+    X, D = W.config_omp_small(5000)
+    Xf, Df = X.astype(np.float32), D.astype(np.float32)
+    _same(spams_b200.omp(Xf, Df, L=10, eps=0.0),
+          spams_b200.omp(Xf, Df, L=10, eps=0.0, refactor="never"))
+
+
+@pytest.mark.parametrize("seed", [4, 5, 6])
+def test_omp_refactor_tracks_the_fp64_path_on_near_duplicate_atoms(seed):
+    """OMP on a dictionary with 50 near-duplicate pairs (correlation ~0.9999):
+    rebuilding the factor in FP64 (on every atom, or on small pivots) keeps
+    the single-precision codes at least as close to the FP64 reference as
+    the incremental updates do; the warp and CTA kernels refactor alike."""
+    D, rng = _near_duplicates(seed)
+    X, _, _ = W.sparse_signals(D, 600, 10, 0.02, rng)
+    ref = O.orc_omp(X, D, L=20, eps=0.05)
+    Xf, Df = X.astype(np.float32), D.astype(np.float32)
+    never = spams_b200.omp(Xf, Df, L=20, eps=0.05, refactor="never")
+    pivot = spams_b200.omp(Xf, Df, L=20, eps=0.05)
+    always = spams_b200.omp(Xf, Df, L=20, eps=0.05, refactor="always")
+    sm = {k: support_match(v, ref) for k, v in (("never", never), ("pivot", pivot),
+                                                 ("always", always))}
+    er = {k: rel_err(v, ref) for k, v in (("never", never), ("pivot", pivot),
+                                           ("always", always))}
+    print(f"\nseed {seed}: support {sm}, rel err {er}")
+    assert sm["always"] >= sm["never"] - 0.002
+    assert er["always"] <= er["never"] * 1.05 + 1e-7
+    assert sm["always"] >= 0.97
+    _same(spams_b200.omp(Xf, Df, L=20, eps=0.05, refactor="always", kernel="warp"),
+          spams_b200.omp(Xf, Df, L=20, eps=0.05, refactor="always", kernel="cta"))
+
+
+def test_lasso_refactor_beyond_32_atoms():
+    """Active sets of more than 32 atoms (refactored up to 96): on every add
+    the codes stay within the single-precision tolerance of FP64."""
+    rng = np.random.Generator(np.random.PCG64(21))
+    D = W.gaussian_dictionary(128, 400, rng)
+    X, _, _ = W.sparse_signals(D, 300, 45, 0.01, rng)
+    ref = O.orc_lasso(X, D, lambda1=0.01)
+    assert (np.diff(ref.indptr) > 32).mean() > 0.5
+    Xf, Df = X.astype(np.float32), D.astype(np.float32)
+    always = spams_b200.lasso(Xf, Df, lambda1=0.01, refactor="always")
+    never = spams_b200.lasso(Xf, Df, lambda1=0.01, refactor="never")
+    print(f"\n>32 atoms: support always {support_match(always, ref):.4f} "
+          f"never {support_match(never, ref):.4f}; rel err always {rel_err(always, ref):.2e} "
+          f"never {rel_err(never, ref):.2e}")
+    assert rel_err(always, ref) <= max(1e-4, 1.05 * rel_err(never, ref))
