@@ -151,8 +151,11 @@ sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K,
  *   L < 0: K; max_length_path < 0: 4L; clamps as the facade.
  *   mode: SC_L1COEFFS / SC_L2ERROR / SC_PENALTY; pos: non-negative codes.
  *   path (optional): K x max_length_path, path of the first signal.
- *   ols / cholesky select the reference's Cholesky variant (lasso<T>,
- *   decomp/decomp.h:735-841); not implemented -> SC_ERR_UNSUPPORTED. */
+ *   ols / cholesky select the reference's Cholesky implementation (lasso<T>
+ *   -> coreLARS + downDateLasso, decomp/decomp.h:735-1203; ols implies it, as
+ *   in _lassoD): its own stopping rules in all three modes, and with ols the
+ *   final least-squares fit on the support.  Up to 1024 atoms
+ *   (SC_ERR_UNSUPPORTED beyond). */
 sc_status sc_lasso_f32(const float* X, int m, int64_t n, const float* D, int K,
                        int L, float lambda1, float lambda2, int mode, int pos,
                        int ols, int numThreads, int max_length_path,
@@ -179,6 +182,22 @@ sc_status sc_lasso_gram_f64(const double* X, int m, int64_t n, const double* Q,
                             double lambda2, int mode, int pos, int numThreads,
                             int max_length_path, double* path,
                             const sc_options* opt, sc_csc_f64* out);
+
+/* The same with _lassoQq's ols / cholevsky arguments (cpp_library/spams.h:
+ * 145-188; ols sets cholevsky, :182-183): the Cholesky implementation
+ * lasso<T>(Data X, G, DtX, ..., ols, ...) (decomp/decomp.h:746-842 ->
+ * coreLARS) on the given products, as for sc_lasso_f32 with cholesky / ols;
+ * with both zero it is sc_lasso_gram_*. */
+sc_status sc_lasso_gram_chol_f32(const float* X, int m, int64_t n, const float* Q, int K,
+                                 const float* q, int L, float lambda1, float lambda2, int mode,
+                                 int pos, int ols, int cholesky, int numThreads,
+                                 int max_length_path, float* path, const sc_options* opt,
+                                 sc_csc_f32* out);
+sc_status sc_lasso_gram_chol_f64(const double* X, int m, int64_t n, const double* Q, int K,
+                                 const double* q, int L, double lambda1, double lambda2, int mode,
+                                 int pos, int ols, int cholesky, int numThreads,
+                                 int max_length_path, double* path, const sc_options* opt,
+                                 sc_csc_f64* out);
 
 /* ---- device-resident variants -------------------------------------------
  * Same computations with X and D in DEVICE memory.  The facade defaults are

@@ -50,12 +50,20 @@ inline sc_status call_lasso(const double* X, int m, int64_t n, const double* D, 
 }
 inline sc_status call_lassoQq(const float* X, int m, int64_t n, const float* Q, int K,
                               const float* q, int L, float l1, float l2, int mode, int pos,
-                              int mlp, float* path, sc_csc_f32* out) {
+                              int mlp, float* path, sc_csc_f32* out, int ols = 0,
+                              int cholesky = 0) {
+  if (ols || cholesky)
+    return sc_lasso_gram_chol_f32(X, m, n, Q, K, q, L, l1, l2, mode, pos, ols, cholesky, -1, mlp,
+                                  path, nullptr, out);
   return sc_lasso_gram_f32(X, m, n, Q, K, q, L, l1, l2, mode, pos, -1, mlp, path, nullptr, out);
 }
 inline sc_status call_lassoQq(const double* X, int m, int64_t n, const double* Q, int K,
                               const double* q, int L, double l1, double l2, int mode, int pos,
-                              int mlp, double* path, sc_csc_f64* out) {
+                              int mlp, double* path, sc_csc_f64* out, int ols = 0,
+                              int cholesky = 0) {
+  if (ols || cholesky)
+    return sc_lasso_gram_chol_f64(X, m, n, Q, K, q, L, l1, l2, mode, pos, ols, cholesky, -1, mlp,
+                                  path, nullptr, out);
   return sc_lasso_gram_f64(X, m, n, Q, K, q, L, l1, l2, mode, pos, -1, mlp, path, nullptr, out);
 }
 inline sc_status call_omp_mask(const float* X, int m, int64_t n, const float* D, int K,
@@ -182,10 +190,9 @@ void lasso2(const Matrix<T>& X, const Matrix<T>& G, const Matrix<T>& DtX, SpMatr
   }
 }
 
-// decomp/decomp.h:735-841: the Cholesky implementation of the same homotopy.
-// In PENALTY and L1COEFFS modes it follows lasso2's path; ols adds the final
-// least-squares fit on the support.  Its L2ERROR rule is not available
-// (the call throws the engine's message).
+// decomp/decomp.h:735-745: the Cholesky implementation (coreLARS +
+// downDateLasso) with its own stopping rules; ols ends with the
+// least-squares fit on the support.  Up to 1024 atoms.
 template <typename T>
 void lasso(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha, int L,
            const T constraint, const T lambda2 = 0, constraint_type mode = PENALTY,
@@ -200,6 +207,30 @@ void lasso(const Matrix<T>& X, const Matrix<T>& D, SpMatrix<T>& spalpha, int L,
   typename d::Csc<T>::type out;
   d::check(d::call_lasso(X.X(), (int)X.m(), n, D.X(), (int)K, L, constraint, lambda2, (int)mode,
                          pos ? 1 : 0, mlp, path ? pbuf.data() : nullptr, &out, ols ? 1 : 0, 1));
+  d::adopt<T>(out, spalpha);
+  if (path) {
+    const size_t cols = std::min<size_t>((size_t)path->n(), (size_t)mlp);
+    for (size_t c = 0; c < cols; ++c)
+      memcpy(path->rawX() + c * path->m(), pbuf.data() + c * K, sizeof(T) * std::min<INTM>(K, path->m()));
+  }
+}
+
+// decomp/decomp.h:746-842: the Cholesky implementation on precomputed
+// G and DtX (used as given); X supplies ||x_i||^2.
+template <typename T>
+void lasso(const Matrix<T>& X, const Matrix<T>& G, const Matrix<T>& DtX, SpMatrix<T>& spalpha,
+           int L, const T lambda, constraint_type mode, const bool pos, const bool ols,
+           const int numThreads = -1, Matrix<T>* path = NULL, const int length_path = -1) {
+  (void)numThreads;
+  namespace d = spams_b200_detail;
+  const INTM n = X.n(), K = G.n();
+  const int Lc = std::min<int>(L, (int)K);
+  const int mlp = length_path <= 1 ? 4 * Lc : length_path;
+  std::vector<T> pbuf(path ? (size_t)K * mlp : 0);
+  typename d::Csc<T>::type out;
+  d::check(d::call_lassoQq(X.X(), (int)X.m(), n, G.X(), (int)K, DtX.X(), L, lambda, T(0),
+                           (int)mode, pos ? 1 : 0, mlp, path ? pbuf.data() : nullptr, &out,
+                           ols ? 1 : 0, 1));
   d::adopt<T>(out, spalpha);
   if (path) {
     const size_t cols = std::min<size_t>((size_t)path->n(), (size_t)mlp);

@@ -48,11 +48,10 @@ SpMatrix<T>* _lassoQq(Matrix<T>* X, Matrix<T>* Q, Matrix<T>* q, Matrix<T>** path
                       int max_length_path, const bool verbose, bool cholevsky) {
   (void)numThreads;
   (void)verbose;
-  (void)cholevsky;
   namespace d = spams_b200_detail;
   if (Q->m() != Q->n()) throw "lasso : Q must be square";
   if (Q->m() != q->m() || X->n() != q->n()) throw "lasso : incompatible matrix dimensions";
-  if (ols) throw "lasso : ols with precomputed (Q, q) is not available in spams_b200";
+  if (ols) cholevsky = ols;  // cpp_library/spams.h:182
   const int K = (int)Q->m();
   const int L0 = L < 0 ? K : L;
   const int mlp = max_length_path < 0 ? 4 * L0 : max_length_path;
@@ -62,7 +61,8 @@ SpMatrix<T>* _lassoQq(Matrix<T>* X, Matrix<T>* Q, Matrix<T>* q, Matrix<T>** path
   typename d::Csc<T>::type out;
   sc_status st = d::call_lassoQq(X->X(), (int)X->m(), X->n(), Q->X(), K, q->X(), L, constraint,
                                  lambda2, (int)mode, pos ? 1 : 0, max_length_path,
-                                 *path ? (*path)->rawX() : nullptr, &out);
+                                 *path ? (*path)->rawX() : nullptr, &out, ols ? 1 : 0,
+                                 cholevsky ? 1 : 0);
   if (st != SC_OK) {
     delete alpha;
     delete *path;

@@ -156,8 +156,8 @@ def ref_lasso(X, D=None, Q=None, q=None, L=-1, lambda1=0.0, lambda2=0.0, mode=2,
     if Q is not None:
         fn = lib.ref_lassoQq_f64 if dt == np.float64 else lib.ref_lassoQq_f32
         fn(_p(X), C.c_int(m), C.c_int(n), _p(Q), C.c_int(K), _p(q), C.c_int(L), ct(lambda1),
-           C.c_int(mode), C.c_int(int(pos)), C.c_int(numThreads), C.c_int(max_length_path),
-           _p(path), C.byref(out))
+           C.c_int(mode), C.c_int(int(pos)), C.c_int(int(ols)), C.c_int(int(cholesky)),
+           C.c_int(numThreads), C.c_int(max_length_path), _p(path), C.byref(out))
     else:
         fn = lib.ref_lasso_f64 if dt == np.float64 else lib.ref_lasso_f32
         fn(_p(X), C.c_int(m), C.c_int(n), _p(D), C.c_int(K), C.c_int(L), ct(lambda1), ct(lambda2),
@@ -225,25 +225,20 @@ def orc_omp(X, D, L=None, eps=None, lambda1=None, return_reg_path=False):
 
 
 def orc_lasso(X, D, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, max_length_path=-1,
-              return_reg_path=False, ols=False, cholesky=False):
-    """C restatement of _lassoD / lasso2 / coreLARS2.
-
-    cholesky / ols select the reference's Cholesky implementation (lasso<T>,
-    coreLARS, decomp/decomp.h:735-1093), which follows the same path in PENALTY
-    and L1COEFFS modes; ols then refits the support by least squares
-    (decomp/decomp.h:1087-1091), done here in numpy.  Its L2ERROR rule differs
-    and is not restated."""
-    if (ols or cholesky) and mode == 1:
-        raise NotImplementedError("the Cholesky variant's L2ERROR rule is not restated")
-    if ols:
-        res = orc_lasso(X, D, L, lambda1, lambda2, mode, pos, max_length_path, return_reg_path)
-        a = res[0] if return_reg_path else res
-        a = ols_refit(a, X, D, max(float(lambda2), 1e-10))
-        return (a, res[1]) if return_reg_path else a
+              return_reg_path=False, ols=False, cholesky=False, Q=None, q=None):
+    """C restatement of _lassoD / _lassoQq: lasso2 / coreLARS2, or with
+    cholesky / ols the Cholesky implementation lasso<T> / coreLARS +
+    downDateLasso (decomp/decomp.h:735-1203).  With Q and q the products are
+    given (Q used as given, X supplies ||x||^2); D is then unused."""
     dt = np.float64 if np.asarray(X).dtype == np.float64 else np.float32
-    X, D = _f(X, dt), _f(D, dt)
+    X = _f(X, dt)
     m, n = X.shape
-    K = D.shape[1]
+    if Q is not None:
+        Q, q = _f(Q, dt), _f(q, dt)
+        K = Q.shape[0]
+    else:
+        D = _f(D, dt)
+        K = D.shape[1]
     lib = _orc_lib()
     ct = C.c_double if dt == np.float64 else C.c_float
     clamp = lib.orc_lasso_clamp_f64 if dt == np.float64 else lib.orc_lasso_clamp_f32
@@ -256,9 +251,20 @@ def orc_lasso(X, D, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False, max_lengt
         return (a, path) if return_reg_path else a
     vM = np.zeros(max(1, Lc * n), dt)
     rM = np.full(max(1, Lc * n), -1, np.int32)
-    fn = lib.orc_lasso_f64 if dt == np.float64 else lib.orc_lasso_f32
-    fn(_p(X), C.c_int(m), C.c_int64(n), _p(D), C.c_int(K), C.c_int(Lc), ct(lambda1), ct(lambda2),
-       C.c_int(mode), C.c_int(int(pos)), C.c_int(mlp.value), _p(vM), _p(rM), _p(path))
+    if ols or cholesky or Q is not None:
+        if not (ols or cholesky):
+            raise NotImplementedError("the restatement takes (Q, q) with the Cholesky variant; "
+                                      "the homotopy computes its products from D")
+        fn = lib.orc_lasso_chol_f64 if dt == np.float64 else lib.orc_lasso_chol_f32
+        fn(_p(X), C.c_int(m), C.c_int64(n), _p(D) if Q is None else None,
+           _p(Q) if Q is not None else None, _p(q) if Q is not None else None, C.c_int(K),
+           C.c_int(Lc), ct(lambda1), ct(lambda2), C.c_int(mode), C.c_int(int(pos)),
+           C.c_int(int(bool(ols))), C.c_int(mlp.value), _p(vM), _p(rM), _p(path))
+    else:
+        fn = lib.orc_lasso_f64 if dt == np.float64 else lib.orc_lasso_f32
+        fn(_p(X), C.c_int(m), C.c_int64(n), _p(D), C.c_int(K), C.c_int(Lc), ct(lambda1),
+           ct(lambda2), C.c_int(mode), C.c_int(int(pos)), C.c_int(mlp.value), _p(vM), _p(rM),
+           _p(path))
     a = _convert(vM, rM, Lc, n, K, dt)
     return (a, path) if return_reg_path else a
 
@@ -362,19 +368,3 @@ def orc_lasso_mask(X, D, B, L=-1, lambda1=0.0, lambda2=0.0, mode=2, pos=False):
     fn(_p(X), C.c_int(m), C.c_int64(n), _p(D), C.c_int(K), _p(Bm), C.c_int(Lc), ct(lambda1),
        ct(lambda2), C.c_int(mode), C.c_int(int(pos)), _p(vM), _p(rM))
     return _convert(vM, rM, Lc, n, K, dt)
-
-
-def ols_refit(A, X, D, ridge):
-    """Least-squares fit of every column of X on its support in A, with the
-    Gram matrix G = D^T D + ridge I in the precision of X (the ols projection
-    of coreLARS, decomp/decomp.h:1087-1091)."""
-    A = A.tocsc().copy()
-    dt = A.dtype
-    Xd, Dd = np.asarray(X, dtype=np.float64), np.asarray(D, dtype=np.float64)
-    G = Dd.T @ Dd + ridge * np.eye(Dd.shape[1])
-    for j in range(A.shape[1]):
-        s, e = A.indptr[j], A.indptr[j + 1]
-        if e > s:
-            idx = A.indices[s:e]
-            A.data[s:e] = np.linalg.solve(G[np.ix_(idx, idx)], Dd[:, idx].T @ Xd[:, j]).astype(dt)
-    return A

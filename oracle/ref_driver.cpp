@@ -117,8 +117,8 @@ static int run_lasso(const T* X, int m, int n, const T* D, int K, int L,
 
 template <typename T>
 static int run_lassoQq(const T* X, int m, int n, const T* Q, int K, const T* q,
-                       int L, T lambda1, int mode, int pos, int numThreads,
-                       int max_length_path, T* path, ref_csc* out) {
+                       int L, T lambda1, int mode, int pos, int ols, int cholesky,
+                       int numThreads, int max_length_path, T* path, ref_csc* out) {
   memset(out, 0, sizeof(*out));
   Matrix<T> mX(const_cast<T*>(X), m, n);
   Matrix<T> mQ(const_cast<T*>(Q), K, K);
@@ -127,8 +127,8 @@ static int run_lassoQq(const T* X, int m, int n, const T* Q, int K, const T* q,
   SpMatrix<T>* a = NULL;
   try {
     a = _lassoQq<T>(&mX, &mQ, &mq, &p, path != NULL, L, lambda1, T(0),
-                    (constraint_type)mode, pos != 0, false, numThreads,
-                    max_length_path, false, false);
+                    (constraint_type)mode, pos != 0, ols != 0, numThreads,
+                    max_length_path, false, cholesky != 0);
   } catch (const char* e) {
     strncpy(out->err, e, sizeof(out->err) - 1);
     return 1;
@@ -323,17 +323,17 @@ int ref_lasso_f32(const float* X, int m, int n, const float* D, int K, int L,
 }
 int ref_lassoQq_f64(const double* X, int m, int n, const double* Q, int K,
                     const double* q, int L, double lambda1, int mode, int pos,
-                    int numThreads, int max_length_path, double* path,
-                    ref_csc* out) {
-  return run_lassoQq<double>(X, m, n, Q, K, q, L, lambda1, mode, pos,
-                             numThreads, max_length_path, path, out);
+                    int ols, int cholesky, int numThreads, int max_length_path,
+                    double* path, ref_csc* out) {
+  return run_lassoQq<double>(X, m, n, Q, K, q, L, lambda1, mode, pos, ols,
+                             cholesky, numThreads, max_length_path, path, out);
 }
 int ref_lassoQq_f32(const float* X, int m, int n, const float* Q, int K,
                     const float* q, int L, float lambda1, int mode, int pos,
-                    int numThreads, int max_length_path, float* path,
-                    ref_csc* out) {
-  return run_lassoQq<float>(X, m, n, Q, K, q, L, lambda1, mode, pos,
-                            numThreads, max_length_path, path, out);
+                    int ols, int cholesky, int numThreads, int max_length_path,
+                    float* path, ref_csc* out) {
+  return run_lassoQq<float>(X, m, n, Q, K, q, L, lambda1, mode, pos, ols,
+                            cholesky, numThreads, max_length_path, path, out);
 }
 
 }  // extern "C"

@@ -297,6 +297,306 @@ int F(orc_lars_signal)(const T* G, int K, T* DtR, T normX, int LL, int mode,
   return cnt;
 }
 
+/* downDateLasso (decomp/decomp.h:1096-1203): drop position mb of the
+ * active set 0..*j of coreLARS's state (all L x L matrices column-major with
+ * leading dimension LL, Gs K x LL).  Decrements *j. */
+static void F(orc_chol_downdate)(int* pj, int mb, T* normX, int ols, int pos, T* Rdn, int* ind,
+                                 T* coeffs, T* sig, T* av, T* Xdn, T* RUn, T* Un, T* Gs,
+                                 T* Gsa, T* Unds, T* R, int LL, int K) {
+  const int j = *pj;
+  const int L = LL;
+  const int indB = ind[mb];
+  if (!pos && sig[mb] < 0) {
+    Rdn[indB] = -Rdn[indB];
+    if (ols) Xdn[indB] = -Xdn[indB];
+  }
+  const int num = j - mb;
+  for (int k = 0; k < num * num; ++k) R[k] = 0;
+  for (int k = 0; k < num; ++k) R[k * num + k] = 1;
+  for (int k = mb + 1; k <= j; ++k) {
+    const T a = -Un[k * L + mb] / Un[mb * L + mb];
+    av[k - mb - 1] = a;
+    for (int r = 0; r < mb; ++r) Un[k * L + r] += a * Un[mb * L + r];
+  }
+  for (int k = mb + 1; k <= j; ++k) {
+    for (int r = 0; r < mb; ++r) Un[(k - 1) * L + r] = Un[k * L + r];
+    for (int r = 0; r < num; ++r) Un[(k - 1) * L + mb + r] = Un[k * L + mb + 1 + r];
+  }
+  T alpha = 1, alphab, gamma;
+  for (int k = 0; k < num; ++k) {
+    alphab = alpha + av[k] * av[k];
+    R[k * num + k] = (T)sqrt((double)(alphab / alpha));
+    gamma = av[k] * R[k * num + k] / alphab;
+    alpha = alphab;
+    for (int r = k + 1; r < num; ++r) R[k * num + r] = gamma * av[r];
+  }
+  if (num > 0) {
+    /* trtri(lower, non-unit): R <- R^-1, column by column */
+    for (int k = 0; k < num; ++k) {
+      R[k * num + k] = (T)1.0 / R[k * num + k];
+      for (int r = k + 1; r < num; ++r) {
+        T s2 = 0;
+        for (int q = k; q < r; ++q) s2 += R[q * num + r] * R[k * num + q];
+        R[k * num + r] = -s2 / R[r * num + r];
+      }
+    }
+    /* trmm(Right, Lower, Trans): Un(0:j, mb:mb+num) <- Un(0:j, mb:mb+num) R^T */
+    for (int r = 0; r < j; ++r)
+      for (int c = num - 1; c >= 0; --c) {
+        T s2 = 0;
+        for (int q = 0; q <= c; ++q) s2 += Un[(mb + q) * L + r] * R[q * num + c];
+        Un[(mb + c) * L + r] = s2;
+      }
+  }
+  /* Unds */
+  for (int k = mb + 1; k <= j; ++k)
+    for (int r = 0; r < j - mb; ++r) Unds[k * L + mb + 1 + r] += av[k - mb - 1] * Unds[mb * L + mb + 1 + r];
+  for (int k = 0; k < mb; ++k)
+    for (int l = mb + 1; l <= j; ++l) Unds[k * L + l - 1] = Unds[k * L + l];
+  for (int k = mb + 1; k <= j; ++k)
+    for (int r = 0; r < j - mb; ++r) Unds[(k - 1) * L + mb + r] = Unds[k * L + mb + 1 + r];
+  if (num > 0) {
+    /* trmm(Right, Lower, Trans) on Unds(mb:j, mb:mb+num), j - mb rows */
+    for (int r = 0; r < j - mb; ++r)
+      for (int c = num - 1; c >= 0; --c) {
+        T s2 = 0;
+        for (int q = 0; q <= c; ++q) s2 += Unds[(mb + q) * L + mb + r] * R[q * num + c];
+        Unds[(mb + c) * L + mb + r] = s2;
+      }
+  }
+  for (int k = mb + 1; k <= j; ++k)
+    for (int l = 0; l < k; ++l) Unds[k * L + l] = 0;
+  /* Gs */
+  for (int k = mb + 1; k <= j; ++k) memcpy(Gs + (size_t)(k - 1) * K, Gs + (size_t)k * K, sizeof(T) * K);
+  if (!pos && sig[mb] < 0)
+    for (int k = 0; k < j; ++k) Gs[(size_t)k * K + indB] = -Gs[(size_t)k * K + indB];
+  /* Gsa */
+  for (int k = mb + 1; k <= j; ++k) {
+    for (int r = 0; r < mb; ++r) Gsa[(k - 1) * L + r] = Gsa[k * L + r];
+    for (int r = 0; r < j - mb; ++r) Gsa[(k - 1) * L + mb + r] = Gsa[k * L + mb + 1 + r];
+  }
+  for (int k = 0; k < mb; ++k)
+    for (int l = mb + 1; l <= j; ++l) Gsa[k * L + l - 1] = Gsa[k * L + l];
+  for (int k = mb + 1; k <= j && !pos; ++k) sig[k - 1] = sig[k];
+  for (int k = mb + 1; k <= j; ++k) ind[k - 1] = ind[k];
+  ind[j] = -1;
+  for (int k = mb + 1; k <= j; ++k) coeffs[k - 1] = coeffs[k];
+  coeffs[j] = 0;
+  if (ols) {
+    for (int k = mb; k <= j; ++k) *normX += RUn[k] * RUn[k];
+    for (int k = mb; k < j; ++k) {
+      RUn[k] = 0;
+      for (int l = 0; l <= k; ++l) RUn[k] += Xdn[ind[l]] * Un[k * L + l];
+      *normX -= RUn[k] * RUn[k];
+    }
+  }
+  *pj = j - 1;
+}
+
+/* coreLARS (decomp/decomp.h:844-1093), the Cholesky implementation of the
+ * Lasso homotopy, for one signal: Rdn (K) = D^T x on entry (overwritten),
+ * ind / coeffs (LL) out, -1 terminated; returns the number of entries. */
+int F(orc_larschol_signal)(const T* G, int K, T* Rdn, T normX, int LL, int mode, T constraint,
+                           int pos, int ols, int length_path, int* ind, T* coeffs, T* path) {
+  for (int k = 0; k < LL; ++k) { coeffs[k] = 0; ind[k] = -1; }
+  if (mode == 1 && normX < constraint) return 0;
+  const int L = ORC_MIN(LL, K);
+  if (length_path <= 1) length_path = 4 * L;
+  const int Lm = LL;  /* leading dimension of the L x L state */
+  T* Xdn = (T*)calloc((size_t)K, sizeof(T));
+  T* A = (T*)calloc((size_t)K, sizeof(T));
+  T* u = (T*)calloc((size_t)Lm, sizeof(T));
+  T* sig = (T*)calloc((size_t)Lm, sizeof(T));
+  T* av = (T*)calloc((size_t)Lm, sizeof(T));
+  T* RUn = (T*)calloc((size_t)Lm, sizeof(T));
+  T* Un = (T*)calloc((size_t)Lm * Lm, sizeof(T));
+  T* Unds = (T*)calloc((size_t)Lm * Lm, sizeof(T));
+  T* Gs = (T*)calloc((size_t)K * Lm, sizeof(T));
+  T* Gsa = (T*)calloc((size_t)Lm * Lm, sizeof(T));
+  T* work = (T*)calloc((size_t)2 * K + Lm, sizeof(T));
+  T* R = (T*)calloc((size_t)Lm * Lm, sizeof(T));
+  const T INF = (T)INFINITY;
+  if (ols) memcpy(Xdn, Rdn, sizeof(T) * K);
+  int cur = pos ? F(orc_argmax)(K, Rdn) : F(orc_iamax)(K, Rdn);
+  int newAtom = 1, iter = 1, j;
+  T Cmax = 0, thrs = 0;
+  for (j = 0; j < L; ++j) {
+    if (newAtom) {
+      ind[j] = cur;
+      if (pos) { Cmax = Rdn[cur]; sig[j] = 1; }
+      else { Cmax = (T)fabs((double)Rdn[cur]); sig[j] = Rdn[cur] < 0 ? (T)-1.0 : (T)1.0; }
+      for (int k = 0; k <= j; ++k) Un[j * Lm + k] = 0;
+      Un[j * Lm + j] = 1;
+      memcpy(Gs + (size_t)K * j, G + (size_t)cur * K, sizeof(T) * K);
+      for (int k = 0; k < j; ++k) Gs[(size_t)K * j + ind[k]] *= sig[k];
+      if (sig[j] < 0) {
+        Rdn[cur] = -Rdn[cur];
+        if (ols) Xdn[cur] = -Xdn[cur];
+        for (int r = 0; r < K; ++r) Gs[(size_t)K * j + r] *= sig[j];
+        for (int k = 0; k <= j; ++k) Gs[cur + (size_t)K * k] *= sig[j];
+      }
+      for (int k = 0; k <= j; ++k) Gsa[j * Lm + k] = Gs[cur + (size_t)K * k];
+      for (int k = 0; k < j; ++k) Gsa[k * Lm + j] = Gsa[j * Lm + k];
+      for (int k = 0; k < j; ++k) Unds[k * Lm + j] = Gsa[j * Lm + k];
+      /* trmv(Upper, Trans, j + 1) on Unds row j (stride Lm) */
+      for (int k = j; k >= 0; --k) {
+        T s2 = 0;
+        for (int l = 0; l <= k; ++l) s2 += Un[k * Lm + l] * Unds[l * Lm + j];
+        work[k] = s2;
+      }
+      for (int k = 0; k <= j; ++k) Unds[k * Lm + j] = work[k];
+      T norm2 = Gsa[j * Lm + j];
+      for (int k = 0; k < j; ++k) norm2 -= Unds[k * Lm + j] * Unds[k * Lm + j];
+      if (norm2 < 1e-15) { ind[j] = -1; break; }
+      Un[j * Lm + j] = -1;
+      for (int k = 0; k < j; ++k) Un[j * Lm + k] = Unds[k * Lm + j];
+      /* trmv(Upper, NoTrans, j) on Un(0:j, j) */
+      for (int r = 0; r < j; ++r) {
+        T s2 = 0;
+        for (int k = r; k < j; ++k) s2 += Un[k * Lm + r] * Un[j * Lm + k];
+        work[r] = s2;
+      }
+      for (int r = 0; r < j; ++r) Un[j * Lm + r] = work[r];
+      const T invNorm = (T)1.0 / (T)sqrt((double)norm2);
+      for (int k = 0; k <= j; ++k) Un[j * Lm + k] *= -invNorm;
+      T d = 0;
+      for (int k = 0; k <= j; ++k) d += Un[j * Lm + k] * Gsa[j * Lm + k];
+      Unds[j * Lm + j] = d;
+    }
+    /* direction: w = Un^T 1, a = 1 / ||w||, u = a Un w */
+    for (int k = j; k >= 0; --k) {
+      T s2 = 0;
+      for (int l = 0; l <= k; ++l) s2 += Un[k * Lm + l];
+      u[k] = s2;
+    }
+    T nr = 0;
+    for (int k = 0; k <= j; ++k) nr += u[k] * u[k];
+    const T a = (T)1.0 / (T)sqrt((double)nr);
+    for (int r = 0; r <= j; ++r) {
+      T s2 = 0;
+      for (int k = r; k <= j; ++k) s2 += Un[k * Lm + r] * u[k];
+      work[r] = s2;
+    }
+    for (int r = 0; r <= j; ++r) u[r] = a * work[r];
+    for (int r = 0; r < K; ++r) {
+      T s2 = 0;
+      for (int k = 0; k <= j; ++k) s2 += Gs[r + (size_t)K * k] * u[k];
+      A[r] = s2;
+    }
+    T potentNorm = 0;
+    if (!ols)
+      for (int k = 0; k <= j; ++k) potentNorm += Rdn[ind[k]] * u[k];
+    if (pos) {
+      for (int k = 0; k < K; ++k) {
+        const T diff = a - A[k];
+        work[k] = diff <= 0 ? INF : (Cmax - Rdn[k]) / diff;
+      }
+      for (int k = 0; k <= j; ++k) work[ind[k]] = INF;
+      for (int k = 0; k < K; ++k) if (work[k] <= 0) work[k] = INF;
+      cur = F(orc_iamin)(K, work);
+    } else {
+      memset(work, 0, sizeof(T) * 2 * K);
+      for (int k = 0; k <= j; ++k) { work[2 * ind[k]] = INF; work[2 * ind[k] + 1] = INF; }
+      for (int k = 0; k < K; ++k) {
+        if (!work[2 * k]) {
+          const T d1 = a - A[k];
+          work[2 * k] = d1 <= 0 ? INF : (Cmax - Rdn[k]) / d1;
+          const T d2 = a + A[k];
+          work[2 * k + 1] = d2 <= 0 ? INF : (Cmax + Rdn[k]) / d2;
+        }
+      }
+      cur = F(orc_iamin)(2 * K, work);
+    }
+    T gamma = work[cur];
+    T gammaMin = 0;
+    int minBasis = 0;
+    if (mode == 2) gamma = ORC_MIN(gamma, (Cmax - constraint) / a);
+    for (int k = 0; k <= j; ++k) work[k] = -(coeffs[k] / u[k]);
+    for (int k = 0; k <= j; ++k) if (coeffs[k] == 0 || work[k] <= 0) work[k] = INF;
+    minBasis = F(orc_iamin)(j + 1, work);
+    gammaMin = work[minBasis];
+    if (gammaMin < gamma) gamma = gammaMin;
+    if (mode == 0) {
+      T Tu = 0;
+      for (int k = 0; k <= j; ++k) Tu += u[k];
+      if (Tu > 10e-10) gamma = ORC_MIN(gamma, (constraint - thrs) / Tu);
+      thrs += gamma * Tu;
+    }
+    if (!ols) {
+      const T t = gamma * gamma - 2 * gamma * potentNorm;
+      if (t > 0 || isnan((double)t) || isinf((double)t)) { ind[j] = -1; break; }
+      normX += t;
+    } else if (newAtom) {
+      RUn[j] = 0;
+      for (int k = 0; k <= j; ++k) RUn[j] += Xdn[ind[k]] * Un[j * Lm + k];
+      normX -= RUn[j] * RUn[j];
+    }
+    for (int k = 0; k <= j; ++k) coeffs[k] += gamma * u[k];
+    if (pos)
+      for (int k = 0; k <= j; ++k) if (coeffs[k] < 0) coeffs[k] = 0;
+    for (int r = 0; r < K; ++r) Rdn[r] += (-gamma) * A[r];
+    if (!pos) cur /= 2;
+    if (path)
+      for (int k = 0; k <= j; ++k) path[(size_t)iter * K + ind[k]] = coeffs[k] * sig[k];
+    if (gamma == gammaMin) {
+      F(orc_chol_downdate)(&j, minBasis, &normX, ols, pos, Rdn, ind, coeffs, sig, av, Xdn, RUn,
+                           Un, Gs, Gsa, Unds, R, Lm, K);
+      newAtom = 0;
+      Cmax = (T)fabs((double)Rdn[ind[0]]);
+      --j;
+    } else {
+      newAtom = 1;
+    }
+    ++iter;
+    if (mode == 2) thrs = (T)fabs((double)Rdn[ind[0]]);
+    if ((j == L - 1) || (mode == 2 && (thrs - constraint < 1e-15)) ||
+        (mode == 0 && (thrs - constraint > -1e-15)) ||
+        (newAtom && mode == 1 && (normX - constraint < 1e-15)) || (normX < 1e-15) ||
+        (iter >= length_path))
+      break;
+  }
+  if (ols) {
+    for (int r = 0; r <= j; ++r) {
+      T s2 = 0;
+      for (int k = r; k <= j; ++k) s2 += Un[k * Lm + r] * RUn[k];
+      work[r] = s2;
+    }
+    for (int r = 0; r <= j; ++r) coeffs[r] = work[r];
+  }
+  for (int k = 0; k <= j && k < LL; ++k) coeffs[k] *= sig[k];
+  free(Xdn); free(A); free(u); free(sig); free(av); free(RUn); free(Un); free(Unds); free(Gs);
+  free(Gsa); free(work); free(R);
+  int cnt = 0;
+  while (cnt < LL && ind[cnt] >= 0) ++cnt;
+  return cnt;
+}
+
+/* lasso<T> with cholesky / ols (decomp/decomp.h:735-842): Gram with the
+ * ridge max(lambda2, 1e-10), or the caller's Q and q (Q used as given). */
+void F(orc_lasso_chol)(const T* X, int m, int64_t n, const T* D, const T* Q, const T* q, int K,
+                       int L, T lambda1, T lambda2, int mode, int pos, int ols, int length_path,
+                       T* vM, int* rM, T* path) {
+  if (L <= 0) return;
+  T* G = (T*)malloc(sizeof(T) * (size_t)K * K);
+  T* Rdn = (T*)malloc(sizeof(T) * (size_t)K);
+  if (Q) {
+    memcpy(G, Q, sizeof(T) * (size_t)K * K);
+  } else {
+    const T ridge = lambda2 > (T)1e-10 ? lambda2 : (T)1e-10;
+    F(orc_gram)(D, m, K, ridge, G);
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const T* x = X + (size_t)i * m;
+    T normX = 0;
+    for (int r = 0; r < m; ++r) normX += x[r] * x[r];
+    if (Q) memcpy(Rdn, q + (size_t)i * K, sizeof(T) * K);
+    else F(orc_dtx)(D, m, K, x, Rdn);
+    F(orc_larschol_signal)(G, K, Rdn, normX, L, mode, lambda1, pos, ols, length_path,
+                           rM + (size_t)i * L, vM + (size_t)i * L, (path && i == 0) ? path : NULL);
+  }
+  free(G); free(Rdn);
+}
+
 /* SpMatrix::convert (linalg/linalg.h:4840-4861): dense L x n (value, row)
  * pairs, -1 terminated per column, to CSC with rows sorted ascending
  * (misc.h:137-166 quicksort; any correct sort gives the same result since

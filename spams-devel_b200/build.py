@@ -41,7 +41,7 @@ def nvcc() -> str:
 
 
 SOURCES = [
-    "csc.cu", "dl.cu", "engine.cu", "gemm.cu", "lars.cu", "lars_cta.cu", "mask.cu",
+    "csc.cu", "dl.cu", "engine.cu", "gemm.cu", "lars.cu", "lars_chol.cu", "lars_cta.cu", "mask.cu",
     "noalloc.cu", "omp.cu", "omp_cta.cu", "refine.cu", "serve.cu", "tc_gemm.cu",
 ]
 

@@ -303,7 +303,8 @@ struct Problem {
   // BF16 hi/lo tensor-core correlations + FP64 refinement (float only)
   bool tc = false;
   bool refine = false;            // FP64 refinement of the final coefficients
-  bool ols = false;               // least-squares refit on the final support (lasso ols)
+  bool ols = false;               // least-squares fit on the final support (lasso ols)
+  bool chol = false;              // the Cholesky implementation (coreLARS, lars_chol.cu)
   int kernel = SC_KERNEL_AUTO;    // SC_KERNEL_*: kernel family (AUTO: tuned)
   int refactor = 1;               // FP64 refactor: 0 never, 1 small pivots, 2 always
   // masked variants (lasso_mask / omp_mask): host row mask m x n, the ridge of
@@ -369,11 +370,15 @@ template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
-  std::vector<Shape> cands = candidates_for<T>(c, p.lars, Kp, p.L, p.kernel);
+  // the Cholesky implementation has one kernel: warps of 4 per block, a
+  // 32-atom state in shared memory, the overflow pass with capacity L
+  std::vector<Shape> cands =
+      p.chol ? std::vector<Shape>{Shape{false, std::min(p.L, 32), 4, 0}}
+             : candidates_for<T>(c, p.lars, Kp, p.L, p.kernel);
   // FP64 refactor of the single-precision state (refactor.cuh): one scratch
   // unit per warp (warp kernels) or CTA (CTA kernels, whose grid is then fixed
   // here)
-  const bool refac = sizeof(T) == 4 && p.refactor != 0;
+  const bool refac = sizeof(T) == 4 && p.refactor != 0 && !p.chol;
   if (refac)
     for (Shape& sh : cands)
       if (sh.cta)
@@ -426,8 +431,9 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     Ovf o;
     o.wpb = sh.cta ? 1 : 4;
     const size_t per =
-        sh.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
-               : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
+        p.chol ? lars_chol_state_bytes(Kp, p.L, sizeof(T))
+        : sh.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
+                 : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
     o.grid = sh.cta ? 2 * c.num_sms : c.num_sms;
     while (o.grid > 1 && (size_t)o.grid * o.wpb * per > ((size_t)256 << 20)) o.grid >>= 1;
     o.bytes = (size_t)o.grid * o.wpb * per;
@@ -679,7 +685,9 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
         a.rf_cap = refactor_cap(shp.Lcap);
         a.rf_units = refac ? rf_units : 0;
-        if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
+        a.ols = p.ols ? 1 : 0;
+        if (p.chol) SC_CUDA(launch_lars_chol<T>(a, shp.grid, shp.wpb, st));
+        else if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
         else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
         if (final_run) pr.launches(1);
         if (may_overflow) {
@@ -688,7 +696,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
           a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
           a.rf_cap = refactor_cap(p.L);
-          if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
+          if (p.chol) SC_CUDA(launch_lars_chol<T>(a, ov.grid, ov.wpb, st));
+          else if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
           else SC_CUDA(launch_lars<T>(a, ov.grid, ov.wpb, st));
         }
       } else {
@@ -732,7 +741,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_TRY(code(shp, cn, true));
     // ---- double-precision solves on the final active sets: the ols
     // projection, or the refinement of single-precision codes
-    if (p.ols || (p.refine && (p.dD || p.dDtX))) {
+    if ((p.ols && !p.chol) || (p.refine && !p.chol && (p.dD || p.dDtX))) {
       pr.mark(ST_REFINE);
       const bool with_level = p.lars && !p.ols;
       const T* q = p.dDtX ? p.dDtX + (size_t)start * p.K : nullptr;
@@ -1060,12 +1069,12 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (mode < 0 || mode > 2)
     return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d not supported by the coding path", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
-  // The Cholesky implementation (lasso<T> / coreLARS, decomp/decomp.h:735-1093)
-  // follows the same path as lasso2 in PENALTY and L1COEFFS modes; its ols
-  // option ends with the least-squares fit on the final support.  Its L2ERROR
-  // stopping rule differs (no exact stop at the constraint) and is not built.
-  if ((ols || cholesky) && mode == SC_L2ERROR)
-    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky variant's L2ERROR rule is not implemented");
+  // ols or cholesky select the Cholesky implementation (lasso<T> / coreLARS,
+  // decomp/decomp.h:735-1093; _lassoD sets cholesky when ols is set), one
+  // warp per signal: dictionaries up to 1024 atoms
+  const bool chol = ols || cholesky;
+  if (chol && K > 1024)
+    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky variant supports up to 1024 atoms (K = %d)", K);
   if (path) memset(path, 0, sizeof(T) * (size_t)K * std::max(0, max_length_path));
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);
@@ -1107,6 +1116,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   p.hX = X; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
   p.ols = ols != 0;
+  p.chol = chol;
   // coreLARS2 replaces a path length <= 1 by 4L (decomp/decomp.h:1722) and
   // writes that many columns; the device buffer covers them, only the
   // caller's max_length_path columns are returned.
@@ -1120,7 +1130,7 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   HostSink<T> sink;
   if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
-  p.refine = want_refine(opt) && std::is_same<T, float>::value;
+  p.refine = want_refine(opt) && std::is_same<T, float>::value && !chol;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
   if (mask) {
@@ -1446,6 +1456,31 @@ sc_status sc_lasso_gram_f64(const double* X, int m, int64_t n, const double* Q, 
   prof_reset();
   return lasso_host<double>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
                             pos, 0, max_length_path, 0, path, opt, out);
+}
+
+sc_status sc_lasso_gram_chol_f32(const float* X, int m, int64_t n, const float* Q, int K,
+                                 const float* q, int L, float lambda1, float lambda2, int mode,
+                                 int pos, int ols, int cholesky, int numThreads,
+                                 int max_length_path, float* path, const sc_options* opt,
+                                 sc_csc_f32* out) {
+  (void)numThreads;
+  if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
+  static const float dummy = 0;
+  prof_reset();
+  return lasso_host<float>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
+                           pos, ols, max_length_path, cholesky, path, opt, out);
+}
+sc_status sc_lasso_gram_chol_f64(const double* X, int m, int64_t n, const double* Q, int K,
+                                 const double* q, int L, double lambda1, double lambda2, int mode,
+                                 int pos, int ols, int cholesky, int numThreads,
+                                 int max_length_path, double* path, const sc_options* opt,
+                                 sc_csc_f64* out) {
+  (void)numThreads;
+  if (!Q && K > 0) return fail(SC_ERR_INVALID_ARG, "lasso : null Q");
+  static const double dummy = 0;
+  prof_reset();
+  return lasso_host<double>(X, m, n, nullptr, Q ? Q : &dummy, q, K, L, lambda1, lambda2, mode,
+                            pos, ols, max_length_path, cholesky, path, opt, out);
 }
 
 sc_status sc_omp_f32_dev(const float* dX, int m, int64_t n, const float* dD, int K, int L,

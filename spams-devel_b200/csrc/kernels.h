@@ -78,6 +78,7 @@ struct LarsArgs {
   int refactor;
   double* rf_scratch;
   int rf_cap, rf_units;
+  int ols;             // Cholesky kernel only: final least-squares fit on the support
 };
 
 template <typename T>
@@ -131,6 +132,14 @@ size_t lars_cta_gstate_bytes(int Lc, int grid);
 // The persistent grid the CTA launcher fills the device with (0 on error).
 template <typename T>
 int lars_cta_grid(int Kp, int Lc, bool gstate);
+
+// The Cholesky implementation of the homotopy (coreLARS + downDateLasso),
+// one warp per signal, Kp <= 1024 (lars_chol.cu); a.gstate set: per-warp
+// state in global slabs of lars_chol_state_bytes(Kp, a.Lcap, sizeof(T)).
+// grid <= 0: as many persistent blocks as fit on the device.
+template <typename T>
+cudaError_t launch_lars_chol(const LarsArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);
+size_t lars_chol_state_bytes(int Kp, int Lc, size_t esz);
 
 template <typename T>
 cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);

@@ -31,7 +31,8 @@ SC_KERNEL_AUTO, SC_KERNEL_WARP, SC_KERNEL_CTA = 0, 1, 2
 EXPORTS = (
     "sc_version", "sc_last_error", "sc_device_count", "sc_csc_free_f32", "sc_csc_free_f64",
     "sc_release_all", "sc_omp_f32", "sc_omp_f64", "sc_lasso_f32", "sc_lasso_f64",
-    "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
+    "sc_lasso_gram_f32", "sc_lasso_gram_f64", "sc_lasso_gram_chol_f32",
+    "sc_lasso_gram_chol_f64", "sc_omp_f32_dev", "sc_lasso_f32_dev",
     "sc_last_profile", "sc_corr_f32_dev", "sc_corr_bf16x3_noalloc_f32",
     "sc_server_create", "sc_server_destroy", "sc_server_add_dictionary_f32",
     "sc_server_remove_dictionary", "sc_server_submit", "sc_server_wait", "sc_server_replay",

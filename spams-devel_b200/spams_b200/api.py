@@ -191,7 +191,12 @@ def lasso(X, D=None, Q=None, q=None, return_reg_path=False, L=-1, lambda1=None, 
     L0 = K if L < 0 else L
     mlp = 4 * L0 if max_length_path < 0 else max_length_path
     path = np.zeros((K, max(mlp, 0)), dtype=dt, order="F") if return_reg_path else None
-    if Q is not None:
+    if Q is not None and (ols or cholesky):
+        fn = _lib.lib().sc_lasso_gram_chol_f64 if f64 else _lib.lib().sc_lasso_gram_chol_f32
+        st = fn(_ptr(X, ct), m, n, _ptr(Q, ct), K, _ptr(q, ct), int(L), float(lambda1),
+                float(lambda2), int(mode), int(bool(pos)), int(bool(ols)), int(bool(cholesky)),
+                numThreads, int(max_length_path), _ptr(path, ct), C.byref(o), C.byref(out))
+    elif Q is not None:
         fn = _lib.lib().sc_lasso_gram_f64 if f64 else _lib.lib().sc_lasso_gram_f32
         st = fn(_ptr(X, ct), m, n, _ptr(Q, ct), K, _ptr(q, ct), int(L), float(lambda1),
                 float(lambda2), int(mode), int(bool(pos)), numThreads, int(max_length_path),

@@ -130,20 +130,42 @@ def gpu_available():
 
 # Golden cases whose float32 solutions are not determined to float32 accuracy:
 # OMP run until L = m atoms (the last picks are made on a residual at
-# rounding level) and LARS with active sets as large as the signal length.
-# For these, single-precision results are checked through the objective
-# value instead of the support.
+# rounding level) and LARS with active sets as large as the signal length
+# (both implementations).  For these, single-precision results are checked
+# through the objective value instead of the support.
 # The L1COEFFS stop of the Cholesky variant also lands within float rounding
 # of the constraint on one column (the reference's float build differs from
 # its double build there too).
-ILL_CONDITIONED = {"omp_L_gt_m", "lasso_dense", "lasso_dense_pos", "lasso_chol_l1"}
+ILL_CONDITIONED = {"omp_L_gt_m", "lasso_dense", "lasso_dense_pos", "lasso_chol_l1",
+                   "lasso_chol_dense", "lasso_chol_dense_pos"}
 
 
-# Cases where the reference's own float build leaves its double result (its
-# float ols projection tracks the residual with cancellation and takes extra
-# atoms on 12% of the columns); single-precision results are compared with
-# the double-precision reference there.
-REF_FLOAT_DIVERGES = {"lasso_ols"}
+# The Cholesky variant's ols in PENALTY mode stops when |Rdn_ind0| - lambda
+# falls below 1e-15 (decomp/decomp.h:1068); without the increment test of
+# the non-ols path it otherwise walks on past lambda.  In single precision
+# that stop is decided at rounding level, so the reference's own float build
+# leaves its double build on up to 37% of these columns.  Single-precision
+# results are held to what ols guarantees whatever the stop: each column is
+# the least-squares fit of x on its own support.
+OLS_FLOAT_UNDETERMINED = {"lasso_ols", "lassoQq_ols", "lasso_ols_dense"}
+
+
+def assert_least_squares_on_support(g, A, tol=2e-3):
+    """D_A^T (x - D_A a) = 0 for every column (relative to ||D_A^T x||)."""
+    X = g["X"].astype(np.float64)
+    if "Q" in g:
+        Gq, Qx = g["Q"].astype(np.float64), g["q"].astype(np.float64)
+    else:
+        D = g["D"].astype(np.float64)
+        Gq, Qx = D.T @ D, D.T @ X
+    A = A.tocsc()
+    for j in range(A.shape[1]):
+        s, e = A.indptr[j], A.indptr[j + 1]
+        if e == s:
+            continue
+        idx = A.indices[s:e]
+        r = Qx[idx, j] - Gq[np.ix_(idx, idx)] @ A.data[s:e].astype(np.float64)
+        assert np.abs(r).max() <= tol * max(1.0, np.abs(Qx[idx, j]).max())
 
 
 def objective(g, A, dt=np.float64):

@@ -1,7 +1,8 @@
 // Drives the drop-in C++ API (include/spams_b200/cppspams.h) the way the
 // reference's own demo drives cppspams.h (cpp_library/test_decomp.cpp:14-64):
 // OMP and LARS-Lasso on a dictionary and a batch of signals, through
-// cppOMP / cppLasso / _omp / _lassoD / lasso2(G, DtX) / _ompMask / _lassoMask.  Inputs and outputs are
+// cppOMP / cppLasso / _omp / _lassoD / lasso2(G, DtX) / lasso(G, DtX) / _lassoQq /
+// _ompMask / _lassoMask.  Inputs and outputs are
 // raw binary files in a directory given on the command line; the GPU test
 // suite compares the outputs with the oracle.
 #include <cstdio>
@@ -97,6 +98,23 @@ static int run(const std::string& dir, int m, int n, int K) {
     SpMatrix<T>* sp2 = cppLasso(X, G, DtX, &path, false, -1, T(0.15));
     write_csc(dir + "/lasso_qq.csc", *sp2);
     delete sp2;
+    // the Cholesky implementation on the same products: lasso(X, G, DtX, ...,
+    // ols) (decomp/decomp.h:746) and _lassoQq with ols (cpp_library/spams.h:145)
+    SpMatrix<T> spc;
+    lasso(X, G, DtX, spc, std::min(m, K), T(1.0), L1COEFFS, false, false);
+    write_csc(dir + "/lasso_gram_chol_l1.csc", spc);
+    SpMatrix<T>* sp3 = _lassoQq(&X, &G, &DtX, &path, false, -1, T(0.05), T(0), L2ERROR, false,
+                                true, -1, -1, false, false);
+    write_csc(dir + "/lasso_qq_ols_l2err.csc", *sp3);
+    delete sp3;
+  }
+  // _lassoD with the Cholesky implementation in L2ERROR mode
+  {
+    Matrix<T>* path = nullptr;
+    SpMatrix<T>* spa = _lassoD(&X, &D, &path, false, -1, T(0.05), T(0), L2ERROR, false, false, -1,
+                               -1, false, true);
+    write_csc(dir + "/lasso_chol_l2err.csc", *spa);
+    delete spa;
   }
   // masked variants: row r of signal i observed unless (7 r + 3 i) % 10 >= 7;
   // signal 0 fully observed, signal 1 not at all

@@ -63,12 +63,23 @@ def cases():
     # the Cholesky implementation (lasso / coreLARS) and its ols projection
     out.append(dict(name="lasso_ols", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.1, ols=True), path=False))
     out.append(dict(name="lasso_chol_l1", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=1.0, mode=0, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_pen", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.15, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_l2err", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.05, mode=1, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_pos", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.1, pos=True, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_path", algo="lasso", X=X[:, :10], D=D, kw=dict(lambda1=0.05, L=12, cholesky=True), path=True))
+    out.append(dict(name="lasso_ols_l2err", algo="lasso", X=X[:, :120], D=D, kw=dict(lambda1=0.05, mode=1, ols=True), path=False))
     # Gaussian signals, LARS runs long with drops (dense active sets, small lambda)
     r = rng(6)
     D = W.gaussian_dictionary(24, 70, r)
     X = np.asfortranarray(r.standard_normal((24, 80)))
     out.append(dict(name="lasso_dense", algo="lasso", X=X, D=D, kw=dict(lambda1=0.01), path=False))
     out.append(dict(name="lasso_dense_pos", algo="lasso", X=X, D=D, kw=dict(lambda1=0.01, pos=True), path=False))
+    # the Cholesky implementation with drops (downDateLasso) in every mode
+    out.append(dict(name="lasso_chol_dense", algo="lasso", X=X, D=D, kw=dict(lambda1=0.01, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_dense_pos", algo="lasso", X=X, D=D, kw=dict(lambda1=0.01, pos=True, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_dense_l2err", algo="lasso", X=X, D=D, kw=dict(lambda1=2.0, mode=1, cholesky=True), path=False))
+    out.append(dict(name="lasso_chol_dense_l1", algo="lasso", X=X, D=D, kw=dict(lambda1=3.0, mode=0, cholesky=True), path=False))
+    out.append(dict(name="lasso_ols_dense", algo="lasso", X=X, D=D, kw=dict(lambda1=0.01, ols=True), path=False))
     # precomputed products (Q, q)
     X, D = W.config_lasso(n=60, seed=7, m=40, K=100, s=6, noise=0.01)
     X = X.astype(np.float32).astype(np.float64)
@@ -76,6 +87,8 @@ def cases():
     Q = D.T @ D
     q = D.T @ X
     out.append(dict(name="lassoQq", algo="lassoQq", X=X, D=D, Q=Q, q=q, kw=dict(lambda1=0.1), path=False))
+    out.append(dict(name="lassoQq_ols", algo="lassoQq", X=X, D=D, Q=Q, q=q, kw=dict(lambda1=0.1, ols=True), path=False))
+    out.append(dict(name="lassoQq_chol_l1", algo="lassoQq", X=X, D=D, Q=Q, q=q, kw=dict(lambda1=1.0, mode=0, cholesky=True), path=False))
     # masked variants: random observed rows (70 %), plus one fully observed,
     # one unobserved and one mostly observed column.  ompMask gets L, eps and
     # lambda explicitly: the reference facade points eps / lambda at an

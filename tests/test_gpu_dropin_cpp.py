@@ -50,7 +50,16 @@ def test_cpp_dropin(tmp_path, std, prec):
         "lasso_pos": O.orc_lasso(X64, D64, lambda1=0.1, pos=True),
         "lasso_gram": O.orc_lasso(X64, D64, lambda1=0.15),
         "lasso_qq": O.orc_lasso(X64, D64, lambda1=0.15),
+        "lasso_chol_l2err": O.orc_lasso(X64, D64, lambda1=0.05, mode=1, cholesky=True),
     }
+    # the Cholesky implementation on the demo's products G (+1e-10) and D^T X,
+    # formed the same way (double sums rounded to the precision)
+    Gq = (D64.T @ D64 + 1e-10 * np.eye(100)).astype(dt).astype(np.float64)
+    qq = (D64.T @ X64).astype(dt).astype(np.float64)
+    cases["lasso_gram_chol_l1"] = O.orc_lasso(X64, None, Q=Gq, q=qq, L=48, lambda1=1.0, mode=0,
+                                              cholesky=True)
+    cases["lasso_qq_ols_l2err"] = O.orc_lasso(X64, None, Q=Gq, q=qq, lambda1=0.05, mode=1,
+                                              ols=True)
     rr, ii = np.meshgrid(np.arange(48), np.arange(400), indexing="ij")
     B = (7 * rr + 3 * ii) % 10 < 7
     B[:, 0] = True
@@ -63,4 +72,5 @@ def test_cpp_dropin(tmp_path, std, prec):
         a = _read_csc(tmp_path / f"{name}.csc")
         assert a.shape == ref.shape, name
         assert support_match(a, ref) >= tol_s, name
-        assert rel_err(a, ref) <= (1e-6 if name in ("lasso_gram", "lasso_qq") and prec == "f64" else tol_v), name
+        gram = name.startswith(("lasso_gram", "lasso_qq"))
+        assert rel_err(a, ref) <= (1e-6 if gram and prec == "f64" else tol_v), name

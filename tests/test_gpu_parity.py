@@ -7,7 +7,8 @@ conditions of the Lasso, least-squares optimality of OMP codes)."""
 import numpy as np
 import pytest
 
-from conftest import (ILL_CONDITIONED, call_kw, golden_csc, golden_names, load_golden,
+from conftest import (ILL_CONDITIONED, OLS_FLOAT_UNDETERMINED, assert_least_squares_on_support,
+                      call_kw, golden_csc, golden_names, load_golden,
                       matched_columns, objective, rel_err, support_match)
 
 import spams_b200
@@ -63,6 +64,9 @@ def test_golden_f32_vs_reference_f64(name):
     a, path = res if "f32_path" in g else (res, None)
     ref = golden_csc(g, "f64")
     assert a.shape == ref.shape
+    if name in OLS_FLOAT_UNDETERMINED:
+        assert_least_squares_on_support(g, a)
+        return
     if name in ILL_CONDITIONED:
         # single precision leaves the FP64 path here (the reference's own
         # float build does too): bound the objective by the worse of the
