@@ -138,7 +138,7 @@ struct sc_dl {
   int L = 0;
   bool profile = false;
   DeviceCtx* ctx = nullptr;
-  Buf G, Xb, split, colptr, rows, vals, cntK, ptrK, fillK, sigK, valK, sigT, valT, scan;
+  Buf G, Xb, split, colptr, rows, vals, cntK, ptrK, fillK, sigK, valK, sigT, valT, scan, tcerr;
 };
 
 extern "C" {
@@ -188,7 +188,7 @@ sc_status sc_dl_destroy(sc_dl* s) {
   cudaSetDevice(s->device);
   if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
   for (Buf* b : {&s->G, &s->Xb, &s->split, &s->colptr, &s->rows, &s->vals, &s->cntK, &s->ptrK,
-                 &s->fillK, &s->sigK, &s->valK, &s->sigT, &s->valT, &s->scan})
+                 &s->fillK, &s->sigK, &s->valK, &s->sigT, &s->valT, &s->scan, &s->tcerr})
     b->release();
   destroy_ctx(s->ctx);
   delete s;
@@ -219,20 +219,25 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   const bool tc = s->precision == SC_PREC_BF16X3;
   const int mp = tc_pad_m(m);
   if (tc) SC_TRY(s->split.reserve((size_t)mp * K * 4));
+  if (tc) SC_TRY(s->tcerr.reserve(256));
 
   // the thread's sc_profile describes this step: its launches always, its
   // coding stages' times when profiling is on
   profile_reset();
   int own_launches = 0;
-  // 1. Gram with the ridge (and the BF16 split of the updated D)
+  // 1. Gram with the ridge: FP32, or in the BF16x3 form from the hi / lo
+  // split of the updated D on the tensor cores
   float* G = reinterpret_cast<float*>(s->G.ptr);
   const float ridge = std::max(s->lambda2, 1e-10f);
-  SC_CUDA(launch_gram<float>(dD, m, K, Kp, ridge, G, st));
-  own_launches += 2;
   if (tc) {
     char* sp = static_cast<char*>(s->split.ptr);
     SC_CUDA(launch_bf16_split(dD, m, m, K, mp, sp, sp + (size_t)mp * K * 2, st));
-    own_launches += 1;
+    SC_CUDA(launch_gram_tc(sp, sp + (size_t)mp * K * 2, mp, K, Kp, ridge, G,
+                           reinterpret_cast<int*>(s->tcerr.ptr), st));
+    own_launches += 3;
+  } else {
+    SC_CUDA(launch_gram<float>(dD, m, K, Kp, ridge, G, st));
+    own_launches += 2;
   }
   // 2. the minibatch
   float* Xb = reinterpret_cast<float*>(s->Xb.ptr);

@@ -899,9 +899,12 @@ static sc_status check_opts(const sc_options* opt) {
 static bool want_tc(const sc_options* opt) { return opt && opt->precision == SC_PREC_BF16X3; }
 static bool want_refine(const sc_options* opt) { return opt && opt->refine > 0; }
 
-// Splits D into its BF16 hi / lo halves for the tensor-core products.
+// Splits D into its BF16 hi / lo halves for the tensor-core products.  With
+// G set, also forms the Gram D^T D + ridge I from the split on the tensor
+// cores (the BF16x3 form computes both products that way).
 template <typename T>
-static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& pr) {
+static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& pr,
+                            T* G = nullptr, T ridge = T(0)) {
   if constexpr (std::is_same<T, float>::value) {
     p.tc = true;
     p.mp = tc_pad_m(p.m);
@@ -910,11 +913,24 @@ static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& 
     p.d_tc_err = misc_at<int>(c.misc, MISC_TC_ERR);
     SC_CUDA(cudaMemsetAsync(p.d_tc_err, 0, 4, st));
     char* ds = reinterpret_cast<char*>(c.dsplit.ptr);
+    pr.mark(ST_GRAM);
     SC_CUDA(launch_bf16_split(p.dD, p.m, p.m, p.K, p.mp, ds, ds + (size_t)p.mp * p.K * 2, st));
     pr.launches(1);
     p.dDsplit = ds;
+    if (G) {
+      SC_CUDA(launch_gram_tc(ds, ds + (size_t)p.mp * p.K * 2, p.mp, p.K, p.Kp, ridge, G,
+                             p.d_tc_err, st));
+      pr.launches(2);
+    }
+  } else {
+    (void)c; (void)st; (void)p; (void)pr; (void)G; (void)ridge;
   }
   return SC_OK;
+}
+// Whether a call forms its products on the tensor cores (BF16x3, float).
+template <typename T>
+static bool tc_form(const sc_options* opt) {
+  return opt && opt->precision == SC_PREC_BF16X3 && std::is_same<T, float>::value;
 }
 
 // After the stream has drained: a tensor-core pipeline wait that gave up.
@@ -984,9 +1000,11 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
-  pr.mark(ST_GRAM);
-  SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, T(0), (T*)c->G.ptr, st));
-  pr.launches(2);
+  if (!tc_form<T>(opt)) {  // (the BF16x3 form computes it with the split below)
+    pr.mark(ST_GRAM);
+    SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, T(0), (T*)c->G.ptr, st));
+    pr.launches(2);
+  }
   // per-signal vectors
   const size_t vbytes = (vecL ? 4 * (size_t)n : 0) + (vecE ? sizeof(T) * (size_t)n : 0) +
                         (vecLa ? sizeof(T) * (size_t)n : 0) + 64;
@@ -1018,7 +1036,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   SC_TRY(c->misc.reserve(MISC_BYTES));
   int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   HostSink<T> sink;
-  if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr, (T*)c->G.ptr, T(0)));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
@@ -1108,9 +1126,11 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
     SC_TRY(c->D.reserve((size_t)m * K * sizeof(T)));
     SC_CUDA(cudaMemcpyAsync(c->D.ptr, D, (size_t)m * K * sizeof(T), cudaMemcpyHostToDevice, st));
     const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);  // MAX(lambda2, 1e-10)
-    pr.mark(ST_GRAM);
-    SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, ridge, (T*)c->G.ptr, st));
-    pr.launches(2);
+    if (!tc_form<T>(opt)) {  // (the BF16x3 form computes it with the split below)
+      pr.mark(ST_GRAM);
+      SC_CUDA(launch_gram<T>((const T*)c->D.ptr, m, K, Kp, ridge, (T*)c->G.ptr, st));
+      pr.launches(2);
+    }
     p.dD = (const T*)c->D.ptr;
   }
   p.hX = X; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
@@ -1129,7 +1149,8 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   SC_TRY(c->misc.reserve(MISC_BYTES));
   int* d_capflag = misc_at<int>(c->misc, MISC_CAPFLAG);
   HostSink<T> sink;
-  if (want_tc(opt) && p.dD) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  if (want_tc(opt) && p.dD)
+    SC_TRY(prepare_tc<T>(*c, st, p, pr, (T*)c->G.ptr, lambda2 > T(1e-10) ? lambda2 : T(1e-10)));
   p.refine = want_refine(opt) && std::is_same<T, float>::value && !chol;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
@@ -1201,14 +1222,16 @@ static sc_status lasso_dev(const T* dX, int m, int64_t n, const T* dD, int K, in
   const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   const T ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
-  pr.mark(ST_GRAM);
-  SC_CUDA(launch_gram<T>(dD, m, K, Kp, ridge, (T*)c->G.ptr, st));
-  pr.launches(2);
+  if (!tc_form<T>(opt)) {  // (the BF16x3 form computes it with the split below)
+    pr.mark(ST_GRAM);
+    SC_CUDA(launch_gram<T>(dD, m, K, Kp, ridge, (T*)c->G.ptr, st));
+    pr.launches(2);
+  }
   Problem<T> p;
   p.lars = true; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.mode = mode; p.lambda1 = lambda1; p.pos = pos; p.length_path = max_length_path;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
-  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr, (T*)c->G.ptr, ridge));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);
@@ -1247,13 +1270,15 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   const int Kp = pad_atoms_for(K, opt);
   SC_TRY(c->G.reserve((size_t)Kp * Kp * sizeof(T)));
   pr.mark(ST_GRAM);
-  SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));
-  pr.launches(2);
+  if (!tc_form<T>(opt)) {  // (the BF16x3 form computes it with the split below)
+    SC_CUDA(launch_gram<T>(dD, m, K, Kp, T(0), (T*)c->G.ptr, st));
+    pr.launches(2);
+  }
   Problem<T> p;
   p.lars = false; p.dX = dX; p.dD = dD; p.m = m; p.n = n; p.K = K; p.Kp = Kp; p.L = L;
   p.Lsig = Lsig; p.eps = eps; p.lambda = lambda; p.dLv = d_L; p.dEps = d_eps; p.dLam = d_lambda;
   p.d_colptr = d_colptr; p.d_rows = d_rows; p.d_vals = d_vals; p.cap = cap;
-  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr));
+  if (want_tc(opt)) SC_TRY(prepare_tc<T>(*c, st, p, pr, (T*)c->G.ptr, T(0)));
   p.refine = want_refine(opt) && std::is_same<T, float>::value;
   p.kernel = opt ? opt->kernel : SC_KERNEL_AUTO;
   p.refactor = !opt || opt->refactor == 0 ? 1 : (opt->refactor > 0 ? 2 : 0);

@@ -121,6 +121,13 @@ __global__ void symmetrize_kernel(T* G, int K, int Kp, T ridge) {
 }
 
 template <typename T>
+cudaError_t launch_symmetrize(T* G, int K, int Kp, T ridge, cudaStream_t st) {
+  const int64_t tot = (int64_t)Kp * Kp;
+  symmetrize_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(G, K, Kp, ridge);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_gram(const T* D, int m, int K, int Kp, T ridge, T* G, cudaStream_t st) {
   cudaError_t e = launch_gemm_tn<T>(D, m, K, D, m, K, m, G, Kp, Kp, st);
   if (e != cudaSuccess) return e;
@@ -170,6 +177,7 @@ cudaError_t launch_pad_rows(const T* src, int K, int64_t ldsrc, int64_t n, T* ds
 template cudaError_t launch_gemm_tn<float>(const float*, int, int, const float*, int, int64_t, int, float*, int, int, cudaStream_t);
 template cudaError_t launch_gemm_tn<double>(const double*, int, int, const double*, int, int64_t, int, double*, int, int, cudaStream_t);
 template cudaError_t launch_gram<float>(const float*, int, int, int, float, float*, cudaStream_t);
+template cudaError_t launch_symmetrize<float>(float*, int, int, float, cudaStream_t);
 template cudaError_t launch_gram<double>(const double*, int, int, int, double, double*, cudaStream_t);
 template cudaError_t launch_colnorms<float>(const float*, int, int64_t, float*, cudaStream_t);
 template cudaError_t launch_colnorms<double>(const double*, int, int64_t, double*, cudaStream_t);

@@ -175,6 +175,10 @@ cudaError_t launch_gemm_tn(const T* A, int lda, int Ka, const T* B, int ldb,
 // zero beyond K.
 template <typename T>
 cudaError_t launch_gram(const T* D, int m, int K, int Kp, T ridge, T* G, cudaStream_t st);
+// Mirror G's upper triangle into the lower one, add the ridge to the first K
+// diagonal entries, zero rows / columns K..Kp-1.
+template <typename T>
+cudaError_t launch_symmetrize(T* G, int K, int Kp, T ridge, cudaStream_t st);
 // norms[i] = ||x_i||^2
 template <typename T>
 cudaError_t launch_colnorms(const T* X, int m, int64_t n, T* norms, cudaStream_t st);
@@ -236,5 +240,9 @@ cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t col
 cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* Xhi,
                            const void* Xlo, int64_t n, int m_pad, int nterms, float* C, int ldc,
                            int rows_out, int* err, cudaStream_t st);
+// G (Kp x Kp) = D^T D + ridge I from the BF16 hi / lo halves of D (m_pad x K
+// each): the 3-term tensor-core product, symmetrised, zero beyond K.
+cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, int Kp, float ridge,
+                           float* G, int* err, cudaStream_t st);
 
 }  // namespace sc

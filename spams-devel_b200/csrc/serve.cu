@@ -39,6 +39,7 @@ struct SrvDict {
   int64_t id = 0;
   int m = 0, K = 0, Kp = 0, mp = 0;
   Buf D, Gomp, Glasso, split;
+  Buf GompTc, GlassoTc, tcerr;  // the Grams of the BF16x3 form (tensor cores)
   size_t bytes = 0;
   int users = 0;  // pending requests and batches in flight
 };
@@ -198,7 +199,8 @@ sc_status run_batch(sc_server* s, Slot& sl, SrvDict& d, std::vector<SrvReq*>& ba
   b.m = d.m;
   b.n = N;
   b.dD = reinterpret_cast<const float*>(d.D.ptr);
-  b.G = reinterpret_cast<const float*>(lars ? d.Glasso.ptr : d.Gomp.ptr);
+  b.G = reinterpret_cast<const float*>(tc ? (lars ? d.GlassoTc.ptr : d.GompTc.ptr)
+                                          : (lars ? d.Glasso.ptr : d.Gomp.ptr));
   b.dDsplit = tc ? d.split.ptr : nullptr;
   b.K = d.K;
   b.Kp = d.Kp;
@@ -474,7 +476,8 @@ sc_status sc_server_destroy(sc_server* s) {
     delete kv.second;
   }
   for (auto& kv : s->dicts)
-    for (Buf* b : {&kv.second->D, &kv.second->Gomp, &kv.second->Glasso, &kv.second->split})
+    for (Buf* b : {&kv.second->D, &kv.second->Gomp, &kv.second->Glasso, &kv.second->split,
+                   &kv.second->GompTc, &kv.second->GlassoTc, &kv.second->tcerr})
       b->release();
   destroy_ctx(s->admin);
   delete s;
@@ -497,7 +500,8 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
       return fail(SC_ERR_INVALID_ARG, "serving: dictionary id %lld exists", (long long)dict_id);
   }
   const size_t gbytes = (size_t)d->Kp * d->Kp * 4;
-  d->bytes = (size_t)m * K * 4 + 2 * gbytes + (size_t)d->mp * K * 4;
+  const bool tcd = tc_gemm_available();
+  d->bytes = (size_t)m * K * 4 + (tcd ? 4 : 2) * gbytes + (size_t)d->mp * K * 4;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->reserved_total() + d->bytes > s->budget)
@@ -513,9 +517,23 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
   const float* dD = reinterpret_cast<const float*>(d->D.ptr);
   SC_CUDA(launch_gram<float>(dD, m, K, d->Kp, 0.f, reinterpret_cast<float*>(d->Gomp.ptr), st));
   SC_CUDA(launch_gram<float>(dD, m, K, d->Kp, 1e-10f, reinterpret_cast<float*>(d->Glasso.ptr), st));
-  if (tc_gemm_available()) {
+  if (tcd) {
+    SC_TRY(d->GompTc.reserve(gbytes));
+    SC_TRY(d->GlassoTc.reserve(gbytes));
+    SC_TRY(d->tcerr.reserve(256));
+    int* err = reinterpret_cast<int*>(d->tcerr.ptr);
+    SC_CUDA(cudaMemsetAsync(err, 0, 4, st));
     char* sp = static_cast<char*>(d->split.ptr);
-    SC_CUDA(launch_bf16_split(dD, m, m, K, d->mp, sp, sp + (size_t)d->mp * K * 2, st));
+    char* lo = sp + (size_t)d->mp * K * 2;
+    SC_CUDA(launch_bf16_split(dD, m, m, K, d->mp, sp, lo, st));
+    SC_CUDA(launch_gram_tc(sp, lo, d->mp, K, d->Kp, 0.f, reinterpret_cast<float*>(d->GompTc.ptr),
+                           err, st));
+    SC_CUDA(launch_gram_tc(sp, lo, d->mp, K, d->Kp, 1e-10f,
+                           reinterpret_cast<float*>(d->GlassoTc.ptr), err, st));
+    int herr = 0;
+    SC_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));
+    SC_CUDA(cudaStreamSynchronize(st));
+    if (herr) return fail(SC_ERR_TIMEOUT, "serving: a bounded tensor-core pipeline wait gave up");
   }
   SC_CUDA(cudaStreamSynchronize(st));
   {
@@ -543,7 +561,8 @@ sc_status sc_server_remove_dictionary(sc_server* s, int64_t dict_id) {
     s->dict_bytes -= d->bytes;
   }
   cudaSetDevice(s->device);
-  for (Buf* b : {&d->D, &d->Gomp, &d->Glasso, &d->split}) b->release();
+  for (Buf* b : {&d->D, &d->Gomp, &d->Glasso, &d->split, &d->GompTc, &d->GlassoTc, &d->tcerr})
+    b->release();
   return SC_OK;
 }
 

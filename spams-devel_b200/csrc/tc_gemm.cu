@@ -346,4 +346,15 @@ cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* 
   return cudaGetLastError();
 }
 
+// G = D^T D (+ ridge on the diagonal) from the BF16 hi / lo halves of D:
+// the correlation product with X = D (3 terms, FP32 accumulation), whose
+// upper triangle is then mirrored (as Matrix::fillSymmetric does after syrk)
+// and whose padding rows / columns are zeroed.  Two launches.
+cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, int Kp, float ridge,
+                           float* G, int* err, cudaStream_t st) {
+  cudaError_t e = launch_tc_corr(Dhi, Dlo, K, Dhi, Dlo, K, m_pad, 3, G, Kp, Kp, err, st);
+  if (e != cudaSuccess) return e;
+  return launch_symmetrize<float>(G, K, Kp, ridge, st);
+}
+
 }  // namespace sc
