@@ -110,6 +110,9 @@ sc_status create_ctx(int device, DeviceCtx** out) {
     SC_CUDA(cudaHostAlloc(&c->pinned_small, 4096, cudaHostAllocDefault));
     SC_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
     SC_CUDA(cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
+    SC_CUDA(cudaStreamCreateWithFlags(&c->lane[1].stream, cudaStreamNonBlocking));
+    SC_CUDA(cudaEventCreateWithFlags(&c->lane[1].done, cudaEventDisableTiming));
+    SC_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     for (int i = 0; i < 2; ++i) {
       SC_CUDA(cudaEventCreateWithFlags(&c->ev_h2d[i], cudaEventDisableTiming));
       SC_CUDA(cudaEventCreateWithFlags(&c->ev_xfree[i], cudaEventDisableTiming));
@@ -131,12 +134,14 @@ void destroy_ctx(DeviceCtx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (cudaStream_t s : {c->h2d_stream, c->d2h_stream})
+  for (cudaStream_t s : {c->h2d_stream, c->d2h_stream, c->lane[1].stream})
     if (s) cudaStreamSynchronize(s);
   for (Buf* b : c->all_bufs()) b->release();
-  for (cudaStream_t s : {c->stream, c->h2d_stream, c->d2h_stream})
+  for (cudaStream_t s : {c->stream, c->h2d_stream, c->d2h_stream, c->lane[1].stream})
     if (s) cudaStreamDestroy(s);
   if (c->last_use) cudaEventDestroy(c->last_use);
+  if (c->lane[1].done) cudaEventDestroy(c->lane[1].done);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   for (int i = 0; i < 2; ++i)
     for (cudaEvent_t e : {c->ev_h2d[i], c->ev_xfree[i], c->ev_out[i], c->ev_d2h[i]})
       if (e) cudaEventDestroy(e);
@@ -391,29 +396,40 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                          (p.tc ? (size_t)p.mp * 4 : 0) +
                          (sink ? (size_t)nbuf * (p.L * (sizeof(T) + 4) + 8) : 0);
   const int64_t nc = chunk_signals(p.n, per_sig, piped);
+  // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i));
+  // with more than one chunk of host signals, chunks alternate between the
+  // two coding lanes (not while profiling, whose stage events need one stream)
+  const ChunkPlan plan = plan_chunks(p.n, nc, piped);
+  const int64_t nchunks = plan.count;
+  const bool dual = piped && !pr.on && nchunks > 1;
+  const int nlanes = dual ? 2 : 1;
 
-  SC_TRY(c.dtx.reserve((size_t)Kp * nc * sizeof(T)));
-  SC_TRY(c.norms.reserve((size_t)nc * sizeof(T)));
-  SC_TRY(c.slab_ind.reserve((size_t)nc * p.L * 4));
-  SC_TRY(c.slab_val.reserve((size_t)nc * p.L * sizeof(T)));
-  SC_TRY(c.cnt.reserve((size_t)nc * 4));
-  SC_TRY(c.ovf_list.reserve((size_t)nc * 8));
   SC_TRY(c.misc.reserve(MISC_BYTES));
   const int64_t scan_len = scan_scratch_len(nc);
-  SC_TRY(c.scan.reserve((size_t)scan_len * 8));
   const size_t xslot = align16((size_t)nc * p.m * sizeof(T));
   if (p.hX) SC_TRY(c.xstage.reserve(xslot * nbuf));
-  if (p.ols || p.refine) {
-    SC_TRY(c.rlist.reserve((size_t)nc * 8));
-    if (p.L > 32) SC_TRY(c.rscratch.reserve(refine_scratch_bytes(p.L, kRefineBigGrid)));
-  }
-  if (p.tc) SC_TRY(c.xsplit.reserve((size_t)nc * p.mp * 4));
-  SC_TRY(c.level.reserve((size_t)nc * sizeof(T)));
   // OMP with per-signal step caps: each launch takes its signals longest first
   const bool ordered = !p.lars && p.dLv && p.L <= kOrderMaxL;
-  if (ordered) {
-    SC_TRY(c.order.reserve((size_t)nc * 8));
-    SC_TRY(c.ordscr.reserve((size_t)(p.L + 1) * 4));
+  for (int li = 0; li < nlanes; ++li) {
+    Lane& W = c.lane[li];
+    SC_TRY(W.dtx.reserve((size_t)Kp * nc * sizeof(T)));
+    SC_TRY(W.norms.reserve((size_t)nc * sizeof(T)));
+    SC_TRY(W.slab_ind.reserve((size_t)nc * p.L * 4));
+    SC_TRY(W.slab_val.reserve((size_t)nc * p.L * sizeof(T)));
+    SC_TRY(W.cnt.reserve((size_t)nc * 4));
+    SC_TRY(W.ovf_list.reserve((size_t)nc * 8));
+    SC_TRY(W.misc.reserve(MISC_BYTES));
+    SC_TRY(W.scan.reserve((size_t)scan_len * 8));
+    if (p.ols || p.refine) {
+      SC_TRY(W.rlist.reserve((size_t)nc * 8));
+      if (p.L > 32) SC_TRY(W.rscratch.reserve(refine_scratch_bytes(p.L, kRefineBigGrid)));
+    }
+    if (p.tc) SC_TRY(W.xsplit.reserve((size_t)nc * p.mp * 4));
+    SC_TRY(W.level.reserve((size_t)nc * sizeof(T)));
+    if (ordered) {
+      SC_TRY(W.order.reserve((size_t)nc * 8));
+      SC_TRY(W.ordscr.reserve((size_t)(p.L + 1) * 4));
+    }
   }
   const size_t col_slot = align16((size_t)(nc + 1) * 8);
   const size_t ent_slot = (size_t)nc * p.L;
@@ -440,7 +456,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     return o;
   };
   for (const Shape& sh : cands)
-    if (sh.Lcap < p.L) SC_TRY(c.gstate.reserve(ovf_plan(sh).bytes));
+    if (sh.Lcap < p.L)
+      for (int li = 0; li < nlanes; ++li) SC_TRY(c.lane[li].gstate.reserve(ovf_plan(sh).bytes));
   // refactor scratch: the largest launch's units, each for the largest
   // refactored active set of any launch
   int rf_units = 0;
@@ -453,7 +470,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       units = std::max(units, (size_t)ov.grid * ov.wpb);
       cap = std::max(cap, refactor_cap(sh.Lcap));
     }
-    SC_TRY(c.rfscr.reserve(units * (size_t)cap * cap * sizeof(double)));
+    for (int li = 0; li < nlanes; ++li)
+      SC_TRY(c.lane[li].rfscr.reserve(units * (size_t)cap * cap * sizeof(double)));
     rf_units = (int)units;
   }
   // masked variants: Dᵀ, the chunk's mask / classes / scaled parameters, and
@@ -482,16 +500,11 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     mk.work = reinterpret_cast<T*>(c.mwork.ptr);
   }
 
-  unsigned* d_counter = misc_at<unsigned>(c.misc, MISC_COUNTERS);
-  int* d_ovf_count = misc_at<int>(c.misc, MISC_OVF_COUNT);
   unsigned long long* d_steps =
-      pr.on ? misc_at<unsigned long long>(c.misc, MISC_STEPS) : nullptr;
+      pr.on ? misc_at<unsigned long long>(c.lane[0].misc, MISC_STEPS) : nullptr;
   if (d_steps) SC_CUDA(cudaMemsetAsync(d_steps, 0, 8, st));
   g_prof.signals += p.n;
 
-  // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i))
-  const ChunkPlan plan = plan_chunks(p.n, nc, piped);
-  const int64_t nchunks = plan.count;
   auto chunk_start = [&](int64_t i) { return plan.start(i); };
   auto chunk_len = [&](int64_t i) { return plan.len(i); };
   auto xslot_ptr = [&](int64_t i) {
@@ -596,11 +609,21 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.last_use, 0));
     SC_TRY(issue_h2d(0));
   }
+  if (dual) {  // lane 1 starts after the call's earlier work on st (the Gram, the split of D)
+    SC_CUDA(cudaEventRecord(c.ev_fork, st));
+    SC_CUDA(cudaStreamWaitEvent(c.lane[1].stream, c.ev_fork, 0));
+  }
+  const cudaStream_t st0 = st;
   for (int64_t ci = 0; ci < nchunks; ++ci) {
     const int64_t start = chunk_start(ci);
     const int64_t cn = chunk_len(ci);
-    T* dtx = reinterpret_cast<T*>(c.dtx.ptr);
-    T* norms = reinterpret_cast<T*>(c.norms.ptr);
+    const int li = dual ? (int)(ci & 1) : 0;
+    Lane& W = c.lane[li];
+    const cudaStream_t st = li ? W.stream : st0;  // this chunk's stream
+    unsigned* d_counter = misc_at<unsigned>(W.misc, MISC_COUNTERS);
+    int* d_ovf_count = misc_at<int>(W.misc, MISC_OVF_COUNT);
+    T* dtx = reinterpret_cast<T*>(W.dtx.ptr);
+    T* norms = reinterpret_cast<T*>(W.norms.ptr);
     // ---- inputs: ||x||^2 and D^T x
     const T* xchunk = nullptr;
     pr.mark(ST_OTHER);
@@ -640,7 +663,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       pr.launches(2);
     } else if (p.tc) {
       if constexpr (std::is_same<T, float>::value) {
-        char* xs = reinterpret_cast<char*>(c.xsplit.ptr);
+        char* xs = reinterpret_cast<char*>(W.xsplit.ptr);
         const size_t half = (size_t)p.mp * cn * 2;
         SC_CUDA(launch_bf16_split(xchunk, p.m, p.m, cn, p.mp, xs, xs + half, st));
         const char* ds = reinterpret_cast<const char*>(p.dDsplit);
@@ -655,18 +678,18 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     // ---- coding (+ rerun of the signals whose active set outgrew Lcap)
     const int64_t* order = nullptr;
     if (ordered) {
-      SC_CUDA(launch_order_by_L_desc(p.dLv + start, cn, p.L, reinterpret_cast<int*>(c.ordscr.ptr),
-                                     reinterpret_cast<int64_t*>(c.order.ptr), st));
+      SC_CUDA(launch_order_by_L_desc(p.dLv + start, cn, p.L, reinterpret_cast<int*>(W.ordscr.ptr),
+                                     reinterpret_cast<int64_t*>(W.order.ptr), st));
       pr.launches(3);
-      order = reinterpret_cast<const int64_t*>(c.order.ptr);
+      order = reinterpret_cast<const int64_t*>(W.order.ptr);
     }
-    int* cnt = reinterpret_cast<int*>(c.cnt.ptr);
-    int* sind = reinterpret_cast<int*>(c.slab_ind.ptr);
-    T* sval = reinterpret_cast<T*>(c.slab_val.ptr);
-    int64_t* ovf_list = reinterpret_cast<int64_t*>(c.ovf_list.ptr);
+    int* cnt = reinterpret_cast<int*>(W.cnt.ptr);
+    int* sind = reinterpret_cast<int*>(W.slab_ind.ptr);
+    T* sval = reinterpret_cast<T*>(W.slab_val.ptr);
+    int64_t* ovf_list = reinterpret_cast<int64_t*>(W.ovf_list.ptr);
     T* path = start == 0 ? p.d_path : nullptr;
     auto code = [&](const Shape& shp, int64_t jobs, bool final_run) -> sc_status {
-      SC_CUDA(cudaMemsetAsync(c.misc.ptr, 0, 64, st));
+      SC_CUDA(cudaMemsetAsync(W.misc.ptr, 0, 64, st));
       const bool may_overflow = shp.Lcap < p.L;
       const Ovf ov = ovf_plan(shp);
       if (p.lars) {
@@ -680,9 +703,9 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.out_cnt = cnt; a.overflow_list = ovf_list; a.overflow_count = d_ovf_count;
         a.gstate = nullptr; a.path = final_run ? path : nullptr;
         a.steps = final_run ? d_steps : nullptr;
-        a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(c.level.ptr) : nullptr;
+        a.out_level = (p.refine && !p.ols) ? reinterpret_cast<T*>(W.level.ptr) : nullptr;
         a.refactor = refac ? p.refactor : 0;
-        a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
+        a.rf_scratch = refac ? reinterpret_cast<double*>(W.rfscr.ptr) : nullptr;
         a.rf_cap = refactor_cap(shp.Lcap);
         a.rf_units = refac ? rf_units : 0;
         a.ols = p.ols ? 1 : 0;
@@ -694,7 +717,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           if (final_run) pr.launches(1);
           a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
-          a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          a.gstate = reinterpret_cast<T*>(W.gstate.ptr);
           a.rf_cap = refactor_cap(p.L);
           if (p.chol) SC_CUDA(launch_lars_chol<T>(a, ov.grid, ov.wpb, st));
           else if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
@@ -714,7 +737,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.path = final_run ? path : nullptr;
         a.steps = final_run ? d_steps : nullptr;
         a.refactor = refac ? p.refactor : 0;
-        a.rf_scratch = refac ? reinterpret_cast<double*>(c.rfscr.ptr) : nullptr;
+        a.rf_scratch = refac ? reinterpret_cast<double*>(W.rfscr.ptr) : nullptr;
         a.rf_cap = refactor_cap(shp.Lcap);
         a.rf_units = refac ? rf_units : 0;
         if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, shp.grid, st));
@@ -724,7 +747,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           if (final_run) pr.launches(1);
           a.Lcap = p.L; a.n_jobs = 0; a.n_jobs_dev = d_ovf_count; a.sig_list = ovf_list;
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
-          a.gstate = reinterpret_cast<T*>(c.gstate.ptr);
+          a.gstate = reinterpret_cast<T*>(W.gstate.ptr);
           a.rf_cap = refactor_cap(p.L);
           if (shp.cta) SC_CUDA(launch_omp_cta<T>(a, ov.grid, st));
           else SC_CUDA(launch_omp<T>(a, ov.grid, ov.wpb, st));
@@ -747,11 +770,11 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       const T* q = p.dDtX ? p.dDtX + (size_t)start * p.K : nullptr;
       SC_CUDA(launch_refine<T>(q ? nullptr : p.dD, p.m, q ? nullptr : xchunk, q, p.K, dG, Kp, sind,
                                sval, p.L, cnt,
-                               with_level ? reinterpret_cast<const T*>(c.level.ptr) : nullptr, cn,
-                               reinterpret_cast<int64_t*>(c.rlist.ptr),
-                               misc_at<int>(c.misc, MISC_RF_COUNT),
-                               misc_at<unsigned>(c.misc, MISC_RF_CTR),
-                               reinterpret_cast<double*>(c.rscratch.ptr), kRefineBigGrid, st));
+                               with_level ? reinterpret_cast<const T*>(W.level.ptr) : nullptr, cn,
+                               reinterpret_cast<int64_t*>(W.rlist.ptr),
+                               misc_at<int>(W.misc, MISC_RF_COUNT),
+                               misc_at<unsigned>(W.misc, MISC_RF_CTR),
+                               reinterpret_cast<double*>(W.rscratch.ptr), kRefineBigGrid, st));
       pr.launches(2);
     }
     if (piped) SC_CUDA(cudaEventRecord(c.ev_xfree[ci & 1], st));  // staging slot free again
@@ -763,7 +786,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     // ---- CSC
     pr.mark(ST_CSC);
     pr.launches(4);
-    int64_t* scratch = reinterpret_cast<int64_t*>(c.scan.ptr);
+    int64_t* scratch = reinterpret_cast<int64_t*>(W.scan.ptr);
     if (sink) {
       const int slot = piped ? (int)(ci & 1) : 0;
       // the read-back of the chunk that used these slots before has ended
@@ -787,6 +810,10 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       SC_CUDA(launch_csc_gather<T>(sind, sval, p.L, cnt, col, cn, nullptr, p.cap, d_capflag,
                                    p.d_rows, p.d_vals, st));
     }
+  }
+  if (dual) {  // the call's stream waits for lane 1's last chunk
+    SC_CUDA(cudaEventRecord(c.lane[1].done, c.lane[1].stream));
+    SC_CUDA(cudaStreamWaitEvent(st, c.lane[1].done, 0));
   }
   if (piped && nchunks > 0) SC_TRY(finalize(nchunks - 1));
   pr.mark(ST_OTHER);

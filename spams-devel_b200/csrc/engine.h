@@ -39,6 +39,21 @@ struct Buf {
   void release();
 };
 
+// Per-chunk workspaces of a coding lane.  Host-array calls code consecutive
+// chunks on two lanes (lane 1 on its own stream), so that one chunk's
+// products and coding start while the previous chunk's persistent grid is
+// still draining; every other call codes on lane 0 in its own stream.
+struct Lane {
+  Buf dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, xsplit, level, rlist, rscratch,
+      gstate, rfscr, order, ordscr;
+  cudaStream_t stream = nullptr;  // lane 1's stream
+  cudaEvent_t done = nullptr;     // end of lane 1's part of a call
+  std::vector<Buf*> bufs() {
+    return {&dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc, &scan, &xsplit, &level,
+            &rlist, &rscratch, &gstate, &rfscr, &order, &ordscr};
+  }
+};
+
 // Per-device state: one stream, cached workspaces.  Calls on one device are
 // serialised by `mu`.
 struct DeviceCtx {
@@ -57,16 +72,17 @@ struct DeviceCtx {
   void* pinned_col = nullptr;  // pinned column pointers of the chunks being read back
   size_t pinned_col_bytes = 0;
   sc_status pinned_cols(size_t bytes);
-  Buf X, D, G, dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, gstate;
-  Buf ccolptr, crows, cvals, path, vecs, xstage, xsplit, dsplit, level, rlist, rscratch;
+  Buf X, D, G, misc;
+  Buf ccolptr, crows, cvals, path, vecs, xstage, dsplit;
   Buf mask, mflag, mvec, Dt, mwork;  // masked variants
-  Buf rfscr;                         // FP64 refactor scratch of the LARS kernels
-  Buf order, ordscr;                 // longest-first signal order of a launch
+  Lane lane[2];
+  cudaEvent_t ev_fork = nullptr;     // lane 1 starts after the call's earlier work
   std::vector<Buf*> all_bufs() {
-    return {&X, &D, &G, &dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc,
-            &scan, &gstate, &ccolptr, &crows, &cvals, &path, &vecs, &xstage, &xsplit,
-            &dsplit, &level, &rlist, &rscratch, &mask, &mflag, &mvec, &Dt, &mwork,
-            &rfscr, &order, &ordscr};
+    std::vector<Buf*> v = {&X, &D, &G, &misc, &ccolptr, &crows, &cvals, &path, &vecs, &xstage,
+                           &dsplit, &mask, &mflag, &mvec, &Dt, &mwork};
+    for (Lane& l : lane)
+      for (Buf* b : l.bufs()) v.push_back(b);
+    return v;
   }
 };
 
