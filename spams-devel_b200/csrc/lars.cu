@@ -316,7 +316,7 @@ lars_kernel(const LarsArgs<T> a) {
         const ScreenBest<T> sb = lars_screen<NV>(A, sDtR + lane * 4, lane * 4, act, C, pos, K);
         const ArgRes<T> mr = warp_argmin_first(sb.key, sb.idx, sb.val);  // warp-uniform
         T step = mr.val;
-        cur = mr.idx % K;
+        cur = join_atom(mr.idx, K);
 
         // ---- polynomial of normX along the step
         T p1 = 0, p2 = 0;

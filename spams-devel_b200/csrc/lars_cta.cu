@@ -259,7 +259,7 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
           for (int w = 1; w < W; ++w)
             if (exK[w] < bk || (exK[w] == bk && exI[w] < bi)) { bk = exK[w]; bi = exI[w]; bv = exV[w]; }
           step = bv;
-          cur = bi % K;
+          cur = join_atom(bi, K);
         }
         // ---- polynomial of normX along the step (every warp, same result)
         T p1 = 0, p2 = 0;

@@ -27,6 +27,13 @@ namespace sc {
 
 template <typename T> struct ScreenBest { T key; T val; int idx; };
 
+// The atom of a joining index in [0, 2K) (index % K without the division);
+// any other index (no candidate at all) maps to atom 0.
+__device__ __forceinline__ int join_atom(int idx, int K) {
+  const unsigned u = (unsigned)idx;
+  return u < (unsigned)K ? idx : (u < 2u * (unsigned)K ? idx - K : 0);
+}
+
 // Reference-exact screen (used in double precision).
 template <int NV>
 __device__ __forceinline__ ScreenBest<double> lars_screen(const double (&A)[NV][4],
