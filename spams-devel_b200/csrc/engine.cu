@@ -393,7 +393,6 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // chunk size: bound D^T X + slabs (+ staged X) to about 2 GiB
   const size_t per_sig = (size_t)Kp * sizeof(T) + (size_t)p.L * (sizeof(T) + 4) + 64 +
                          (p.hX ? (size_t)nbuf * p.m * sizeof(T) : 0) +
-                         (p.tc ? (size_t)p.mp * 4 : 0) +
                          (sink ? (size_t)nbuf * (p.L * (sizeof(T) + 4) + 8) : 0);
   const int64_t nc = chunk_signals(p.n, per_sig, piped);
   // chunk i covers signals [chunk_start(i), chunk_start(i) + chunk_len(i));
@@ -424,7 +423,6 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       SC_TRY(W.rlist.reserve((size_t)nc * 8));
       if (p.L > 32) SC_TRY(W.rscratch.reserve(refine_scratch_bytes(p.L, kRefineBigGrid)));
     }
-    if (p.tc) SC_TRY(W.xsplit.reserve((size_t)nc * p.mp * 4));
     SC_TRY(W.level.reserve((size_t)nc * sizeof(T)));
     if (ordered) {
       SC_TRY(W.order.reserve((size_t)nc * 8));
@@ -663,13 +661,11 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       pr.launches(2);
     } else if (p.tc) {
       if constexpr (std::is_same<T, float>::value) {
-        char* xs = reinterpret_cast<char*>(W.xsplit.ptr);
-        const size_t half = (size_t)p.mp * cn * 2;
-        SC_CUDA(launch_bf16_split(xchunk, p.m, p.m, cn, p.mp, xs, xs + half, st));
+        // BF16 hi / lo products with the split of X done inside the kernel
         const char* ds = reinterpret_cast<const char*>(p.dDsplit);
-        SC_CUDA(launch_tc_corr(ds, ds + (size_t)p.mp * p.K * 2, p.K, xs, xs + half, cn, p.mp, 3,
-                               dtx, Kp, Kp, p.d_tc_err, st));
-        pr.launches(3);
+        SC_CUDA(launch_tc_corr_fused(ds, ds + (size_t)p.mp * p.K * 2, p.K, xchunk, p.m, p.m, cn,
+                                     p.mp, dtx, Kp, Kp, p.d_tc_err, st));
+        pr.launches(1);
       }
     } else {
       SC_CUDA(launch_gemm_tn<T>(p.dD, p.m, p.K, xchunk, p.m, cn, p.m, dtx, Kp, Kp, st));
@@ -1563,16 +1559,13 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
   if (!tc_gemm_available()) return fail(SC_ERR_UNSUPPORTED, "corr : tensor-map encoder unavailable");
   const int mp = tc_pad_m(m);
   SC_TRY(c->D.reserve((size_t)mp * K * 4));  // hi + lo
-  SC_TRY(c->xstage.reserve((size_t)mp * n * 4));
   SC_TRY(c->misc.reserve(MISC_BYTES));
   int* d_err = misc_at<int>(c->misc, MISC_TC_ERR);
   char* dh = (char*)c->D.ptr;
-  char* xh = (char*)c->xstage.ptr;
   SC_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
   SC_CUDA(launch_bf16_split(dD, m, m, K, mp, dh, dh + (size_t)mp * K * 2, st));
-  SC_CUDA(launch_bf16_split(dX, m, m, n, mp, xh, xh + (size_t)mp * n * 2, st));
-  SC_CUDA(launch_tc_corr(dh, dh + (size_t)mp * K * 2, K, xh, xh + (size_t)mp * n * 2, n, mp, 3,
-                         dC, ldc, K, d_err, st));
+  SC_CUDA(launch_tc_corr_fused(dh, dh + (size_t)mp * K * 2, K, dX, m, m, n, mp, dC, ldc, K, d_err,
+                               st));
   int* h = reinterpret_cast<int*>(c->pinned_small);
   SC_CUDA(cudaMemcpyAsync(h, d_err, 4, cudaMemcpyDeviceToHost, st));
   SC_CUDA(cudaStreamSynchronize(st));

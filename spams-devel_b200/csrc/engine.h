@@ -44,12 +44,12 @@ struct Buf {
 // products and coding start while the previous chunk's persistent grid is
 // still draining; every other call codes on lane 0 in its own stream.
 struct Lane {
-  Buf dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, xsplit, level, rlist, rscratch,
+  Buf dtx, norms, slab_ind, slab_val, cnt, ovf_list, misc, scan, level, rlist, rscratch,
       gstate, rfscr, order, ordscr;
   cudaStream_t stream = nullptr;  // lane 1's stream
   cudaEvent_t done = nullptr;     // end of lane 1's part of a call
   std::vector<Buf*> bufs() {
-    return {&dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc, &scan, &xsplit, &level,
+    return {&dtx, &norms, &slab_ind, &slab_val, &cnt, &ovf_list, &misc, &scan, &level,
             &rlist, &rscratch, &gstate, &rfscr, &order, &ordscr};
   }
 };

@@ -240,6 +240,11 @@ cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t col
 cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* Xhi,
                            const void* Xlo, int64_t n, int m_pad, int nterms, float* C, int ldc,
                            int rows_out, int* err, cudaStream_t st);
+// The same product for fp32 X (m x n, ld ldx >= m) with the split of X done
+// inside the kernel (persistent, one CTA per SM, two TMEM accumulators).
+cudaError_t launch_tc_corr_fused(const void* Dhi, const void* Dlo, int K, const float* X,
+                                 int64_t ldx, int m, int64_t n, int m_pad, float* C, int ldc,
+                                 int rows_out, int* err, cudaStream_t st);
 // G (Kp x Kp) = D^T D + ridge I from the BF16 hi / lo halves of D (m_pad x K
 // each): the 3-term tensor-core product, symmetrised, zero beyond K.
 cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, int Kp, float ridge,

@@ -232,6 +232,254 @@ tc_corr_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ 
                  : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form with the split of X fused in: C = D^T X for fp32 X.
+//
+// One CTA per SM loops over 128-atom x 128-signal output tiles (consecutive
+// tiles of a CTA share their signals, so X is read from HBM once and from L2
+// for the other atom tiles).  Per 64-deep k-block a stage holds Dhi and Dlo
+// (TMA, 128-byte swizzle) and Xhi and Xlo, which four converter warps write
+// from the fp32 signals in the same swizzled layout (the 16-byte chunk j of
+// row r at chunk j ^ (r & 7) of the row's 128-byte line), so no split copy of
+// X exists in memory.  The MMA thread issues the three products of the
+// k-block (Dhi Xhi, Dhi Xlo, Dlo Xhi) into one of two TMEM accumulators;
+// four epilogue warps read the other accumulator with tcgen05.ld and store
+// its tile while the next one is multiplied.
+//   warps 0-3  convert X          warps 4-7  epilogue (TMEM lanes 0-127)
+//   warp 8     TMA of D           warp 9     MMA issue
+// Every wait is bounded: on timeout the CTA records an error, stops issuing
+// work, waits for what it issued and frees its TMEM.
+constexpr int T2_STAGES = 3;
+constexpr int T2_TILE_BYTES = TC_BM * TC_BK * 2;  // 16 KB: one 128 x 64 bf16 operand tile
+constexpr int T2_STAGE_BYTES = 4 * T2_TILE_BYTES; // Dhi | Dlo | Xhi | Xlo
+constexpr int T2_TMEM_COLS = 2 * TC_BN;           // two 128-column accumulators
+constexpr int T2_THREADS = 320;
+constexpr size_t T2_SMEM = (size_t)T2_STAGES * T2_STAGE_BYTES + 1024 + 256;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(T2_THREADS, 1)
+tc_corr_fused_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                     const float* __restrict__ X, int64_t ldx, int m, int64_t n, int m_pad,
+                     float* __restrict__ C, int ldc, int rows_out, int m_tiles, int64_t n_tiles,
+                     int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + T2_STAGES * T2_STAGE_BYTES);
+  // bars: full[S], empty[S], acc_full[2], acc_empty[2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * T2_STAGES + 4);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (T2_STAGES + s); };
+  auto accf_bar = [&](int b) { return bar0 + 8u * (2 * T2_STAGES + b); };
+  auto acce_bar = [&](int b) { return bar0 + 8u * (2 * T2_STAGES + 2 + b); };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < T2_STAGES; ++s) {
+      mbar_init(full_bar(s), 5);   // four converter warps + the TMA thread (with its bytes)
+      mbar_init(empty_bar(s), 1);  // tcgen05.commit
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf_bar(b), 1);   // tcgen05.commit
+      mbar_init(acce_bar(b), 4);   // four epilogue warps
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(T2_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int kblocks = m_pad / TC_BK;
+  const int64_t tiles = (int64_t)m_tiles * n_tiles;
+
+  if (warp < 4) {
+    // ---- converter: Xhi / Xlo of every k-block of the tile's 128 signals
+    int64_t kbg = 0;
+    for (int64_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+      const int64_t n0 = (t / m_tiles) * TC_BN;
+      for (int kb = 0; kb < kblocks; ++kb, ++kbg) {
+        const int s = (int)(kbg % T2_STAGES);
+        const uint32_t round = (uint32_t)(kbg / T2_STAGES);
+        // every lane waits; the warp goes on only if all of them saw the phase
+        if (!__all_sync(kFull, mbar_wait(empty_bar(s), (round & 1u) ^ 1u))) {
+          *abort_flag = 1;
+          break;
+        }
+        uint8_t* xh = smem + (size_t)s * T2_STAGE_BYTES + 2 * T2_TILE_BYTES;
+        uint8_t* xl = xh + T2_TILE_BYTES;
+        const int k0 = kb * TC_BK;
+        // 128 rows x 8 chunks of 8 values: unit u = threadIdx.x + 128 q
+        float v[8][8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int u = threadIdx.x + 128 * q;
+          const int row = u >> 3, ch = u & 7;
+          const int64_t sig = n0 + row;
+          const int k = k0 + ch * 8;
+          if (VEC && sig < n && k + 8 <= m) {
+            const float* src = X + (size_t)sig * ldx + k;
+            const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(src + 4));
+            v[q][0] = a.x; v[q][1] = a.y; v[q][2] = a.z; v[q][3] = a.w;
+            v[q][4] = b.x; v[q][5] = b.y; v[q][6] = b.z; v[q][7] = b.w;
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+              v[q][e] = (sig < n && k + e < m) ? X[(size_t)sig * ldx + k + e] : 0.f;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int u = threadIdx.x + 128 * q;
+          const int row = u >> 3, ch = u & 7;
+          __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            h[e] = __float2bfloat16_rn(v[q][e]);
+            l[e] = __float2bfloat16_rn(v[q][e] - __bfloat162float(h[e]));
+          }
+          const uint32_t off = (uint32_t)row * 128u + ((uint32_t)(ch ^ (row & 7)) << 4);
+          *reinterpret_cast<uint4*>(xh + off) = *reinterpret_cast<const uint4*>(h);
+          *reinterpret_cast<uint4*>(xl + off) = *reinterpret_cast<const uint4*>(l);
+        }
+        // make the generic-proxy writes visible to the tensor cores, then arrive
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(full_bar(s));
+      }
+    }
+  } else if (warp < 8) {
+    // ---- epilogue: TMEM -> registers -> C (column-major, atoms contiguous)
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int b = it & 1;
+      if (*abort_flag || !__all_sync(kFull, mbar_wait(accf_bar(b), (uint32_t)(it >> 1) & 1u))) {
+        *abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int m0 = (int)(t % m_tiles) * TC_BM;
+      const int64_t n0 = (t / m_tiles) * TC_BN;
+      const int wl = warp & 3;  // TMEM lanes 32 wl .. 32 wl + 31
+      const int row = m0 + wl * 32 + lane;
+#pragma unroll 1
+      for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t taddr = tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)(b * TC_BN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+              "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+              "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+              "=r"(v[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < rows_out) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int64_t col = n0 + c0 + j;
+            if (col < n) C[(size_t)col * ldc + row] = __uint_as_float(v[j]);
+          }
+        }
+      }
+      // the accumulator may take the next tile
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce_bar(b));
+    }
+  } else if (warp == 8) {
+    // ---- TMA producer of the D halves
+    if (lane == 0) {
+      int64_t kbg = 0, issued = 0;
+      for (int64_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+        const int m0 = (int)(t % m_tiles) * TC_BM;
+        for (int kb = 0; kb < kblocks; ++kb, ++kbg) {
+          const int s = (int)(kbg % T2_STAGES);
+          const uint32_t round = (uint32_t)(kbg / T2_STAGES);
+          if (*abort_flag || !mbar_wait(empty_bar(s), (round & 1u) ^ 1u)) { *abort_flag = 1; break; }
+          uint8_t* st = smem + (size_t)s * T2_STAGE_BYTES;
+          mbar_expect_tx(full_bar(s), 2 * T2_TILE_BYTES);
+          tma_load_2d(smem_u32(st), &mAh, full_bar(s), kb * TC_BK, m0);
+          tma_load_2d(smem_u32(st + T2_TILE_BYTES), &mAl, full_bar(s), kb * TC_BK, m0);
+          issued = kbg + 1;
+        }
+      }
+      if (*abort_flag) {
+        // the copies of the last stages must land before the CTA may exit
+        for (int64_t k = issued - T2_STAGES < 0 ? 0 : issued - T2_STAGES; k < issued; ++k)
+          mbar_wait(full_bar((int)(k % T2_STAGES)), (uint32_t)(k / T2_STAGES) & 1u);
+      }
+    }
+  } else {
+    // ---- MMA issuer
+    if (lane == 0) {
+      int64_t kbg = 0;
+      int it = 0;
+      bool any = false;
+      for (int64_t t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, ++it) {
+        const int b = it & 1;
+        if (!mbar_wait(acce_bar(b), ((uint32_t)(it >> 1) & 1u) ^ 1u)) { *abort_flag = 1; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * TC_BN);
+        for (int kb = 0; kb < kblocks; ++kb, ++kbg) {
+          const int s = (int)(kbg % T2_STAGES);
+          const uint32_t round = (uint32_t)(kbg / T2_STAGES);
+          if (*abort_flag || !mbar_wait(full_bar(s), round & 1u)) { *abort_flag = 1; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t dh = smem_u32(smem + (size_t)s * T2_STAGE_BYTES);
+          const uint32_t dl = dh + T2_TILE_BYTES, xh = dh + 2 * T2_TILE_BYTES,
+                         xl = dh + 3 * T2_TILE_BYTES;
+#pragma unroll
+          for (int k = 0; k < TC_BK / 16; ++k) {
+            const uint32_t o = 32u * k;
+            umma_bf16(acc, sw128_desc(dh + o), sw128_desc(xh + o), (kb > 0 || k > 0) ? 1u : 0u);
+            umma_bf16(acc, sw128_desc(dh + o), sw128_desc(xl + o), 1u);
+            umma_bf16(acc, sw128_desc(dl + o), sw128_desc(xh + o), 1u);
+          }
+          umma_commit(empty_bar(s));  // the stage is free once these have read it
+          any = true;
+        }
+        if (*abort_flag) break;
+        umma_commit(accf_bar(b));  // the tile's accumulator is complete
+      }
+      if (*abort_flag && any) {
+        // every issued MMA has finished before TMEM is freed: a last commit
+        // arrives on an accumulator barrier once all earlier ones are done
+        umma_commit(accf_bar(it & 1));
+        mbar_wait(accf_bar(it & 1), (uint32_t)(it >> 1) & 1u);
+      }
+    }
+  }
+  __syncwarp();
+  if (*abort_flag && threadIdx.x == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(T2_TMEM_COLS)
+                 : "memory");
+}
+
 // x (rows x cols, ld ldx, fp32) -> hi, lo (rows_pad x cols, bf16), zero rows
 // beyond `rows`.  One thread converts 8 consecutive rows of a column (two
 // 16-byte loads when the column is 16-byte aligned, two 16-byte stores).
@@ -355,6 +603,40 @@ cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, i
   cudaError_t e = launch_tc_corr(Dhi, Dlo, K, Dhi, Dlo, K, m_pad, 3, G, Kp, Kp, err, st);
   if (e != cudaSuccess) return e;
   return launch_symmetrize<float>(G, K, Kp, ridge, st);
+}
+
+cudaError_t launch_tc_corr_fused(const void* Dhi, const void* Dlo, int K, const float* X,
+                                 int64_t ldx, int m, int64_t n, int m_pad, float* C, int ldc,
+                                 int rows_out, int* err, cudaStream_t st) {
+  if (n <= 0 || K <= 0) return cudaSuccess;
+  if (!load_encode()) return cudaErrorNotSupported;
+  const int Kp = ((K + TC_BM - 1) / TC_BM) * TC_BM;
+  if (m <= 0 || m_pad % TC_BK != 0 || m > m_pad || ldx < m || ldc < rows_out || !X || !C)
+    return cudaErrorInvalidValue;
+  if (rows_out > Kp) {  // rows past the last tile (a wider padding of K) are zero
+    cudaError_t e = cudaMemset2DAsync(C + Kp, (size_t)ldc * sizeof(float), 0,
+                                      (size_t)(rows_out - Kp) * sizeof(float), (size_t)n, st);
+    if (e != cudaSuccess) return e;
+    rows_out = Kp;
+  }
+  CUtensorMap mAh, mAl;
+  if (!make_map(&mAh, Dhi, m_pad, K, TC_BM) || !make_map(&mAl, Dlo, m_pad, K, TC_BM))
+    return cudaErrorInvalidValue;
+  const int m_tiles = Kp / TC_BM;
+  const int64_t n_tiles = (n + TC_BN - 1) / TC_BN;
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int64_t tiles = (int64_t)m_tiles * n_tiles;
+  const unsigned grid = (unsigned)std::min<int64_t>(tiles, sms > 0 ? sms : 1);
+  const bool vec = (ldx % 4 == 0) && (((uintptr_t)X & 15u) == 0);
+  auto k = vec ? tc_corr_fused_kernel<true> : tc_corr_fused_kernel<false>;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T2_SMEM);
+  if (e != cudaSuccess) return e;
+  k<<<grid, T2_THREADS, T2_SMEM, st>>>(mAh, mAl, X, ldx, m, n, m_pad, C, ldc, rows_out, m_tiles,
+                                         n_tiles, err);
+  return cudaGetLastError();
 }
 
 }  // namespace sc
