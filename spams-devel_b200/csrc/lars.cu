@@ -122,7 +122,11 @@ __device__ __forceinline__ void lane_loop(int n, F&& f) {
 // 2.42 -> 2.22 ms on the 100k-signal lasso workload); -1 reads it from a.
 // SMALL (active-set capacity at most 32) turns the loops over the active set
 // into one guarded pass per lane (2.19 -> 2.03 ms on the same workload).
-template <typename T, int NV, bool MASKED = false, int MODE = -1, bool SMALL = false>
+// GSTATE = false: the state is known to live in shared memory (the main pass
+// with a small active-set capacity), so every state access compiles to a
+// 32-bit shared-space load or store instead of a generic one.
+template <typename T, int NV, bool MASKED = false, int MODE = -1, bool SMALL = false,
+          bool GSTATE = true>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 lars_kernel(const LarsArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,9 +137,9 @@ lars_kernel(const LarsArgs<T> a) {
   const int ldi = state_ld(Lc);
   const size_t per_warp = lars_state_bytes(a.Kp, Lc, sizeof(T));
   unsigned char* base =
-      a.gstate ? reinterpret_cast<unsigned char*>(a.gstate) +
-                     (size_t)(blockIdx.x * wpb + wib) * per_warp
-               : smem_raw + (size_t)wib * per_warp;
+      (GSTATE && a.gstate) ? reinterpret_cast<unsigned char*>(a.gstate) +
+                                 (size_t)(blockIdx.x * wpb + wib) * per_warp
+                           : smem_raw + (size_t)wib * per_warp;
   T* sDtR = reinterpret_cast<T*>(base);
   T* sInv = sDtR + a.Kp;
   T* sU = sInv + (size_t)Lc * ldi;
@@ -419,10 +423,10 @@ template <typename T, int NV>
 static cudaError_t launch_nv(const LarsArgs<T>& a, int grid, int warps_per_block,
                              size_t smem, cudaStream_t st) {
   const bool penalty = a.mode == 2 && !a.pos;
-  auto k = a.mk.mask              ? lars_kernel<T, NV, true>
-           : penalty && a.Lcap <= 32 ? lars_kernel<T, NV, false, 2, true>
-           : penalty               ? lars_kernel<T, NV, false, 2>
-                                   : lars_kernel<T, NV, false>;
+  auto k = a.mk.mask                          ? lars_kernel<T, NV, true>
+           : penalty && a.Lcap <= 32 && !a.gstate ? lars_kernel<T, NV, false, 2, true, false>
+           : penalty                           ? lars_kernel<T, NV, false, 2>
+                                               : lars_kernel<T, NV, false>;
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   k<<<grid, warps_per_block * 32, smem, st>>>(a);
