@@ -218,21 +218,22 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
   SC_TRY(s->scan.reserve((size_t)slen * 8));
   const bool tc = s->precision == SC_PREC_BF16X3;
   const int mp = tc_pad_m(m);
-  if (tc) SC_TRY(s->split.reserve((size_t)mp * K * 4));
+  if (tc) SC_TRY(s->split.reserve((size_t)mp * K * 6));  // hi, lo, lo3 pieces of D
   if (tc) SC_TRY(s->tcerr.reserve(256));
 
   // the thread's sc_profile describes this step: its launches always, its
   // coding stages' times when profiling is on
   profile_reset();
   int own_launches = 0;
-  // 1. Gram with the ridge: FP32, or in the BF16x3 form from the hi / lo
-  // split of the updated D on the tensor cores
+  // 1. Gram with the ridge: FP32, or in the BF16x3 form from the three-piece
+  // split of the updated D on the tensor cores (FP32-grade)
   float* G = reinterpret_cast<float*>(s->G.ptr);
   const float ridge = std::max(s->lambda2, 1e-10f);
   if (tc) {
     char* sp = static_cast<char*>(s->split.ptr);
-    SC_CUDA(launch_bf16_split(dD, m, m, K, mp, sp, sp + (size_t)mp * K * 2, st));
-    SC_CUDA(launch_gram_tc(sp, sp + (size_t)mp * K * 2, mp, K, Kp, ridge, G,
+    const size_t piece = (size_t)mp * K * 2;
+    SC_CUDA(launch_bf16_split(dD, m, m, K, mp, sp, sp + piece, st, sp + 2 * piece));
+    SC_CUDA(launch_gram_tc(sp, sp + piece, sp + 2 * piece, mp, K, Kp, ridge, G,
                            reinterpret_cast<int*>(s->tcerr.ptr), st));
     own_launches += 3;
   } else {

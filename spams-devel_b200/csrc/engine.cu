@@ -923,25 +923,28 @@ static bool want_tc(const sc_options* opt) { return opt && opt->precision == SC_
 static bool want_refine(const sc_options* opt) { return opt && opt->refine > 0; }
 
 // Splits D into its BF16 hi / lo halves for the tensor-core products.  With
-// G set, also forms the Gram D^T D + ridge I from the split on the tensor
-// cores (the BF16x3 form computes both products that way).
+// G set, also a third piece lo3 = bf16(d - hi - lo), from which the Gram
+// D^T D + ridge I is formed on the tensor cores to FP32 grade (the BF16x3
+// form computes both products that way).
 template <typename T>
 static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& pr,
                             T* G = nullptr, T ridge = T(0)) {
   if constexpr (std::is_same<T, float>::value) {
     p.tc = true;
     p.mp = tc_pad_m(p.m);
-    SC_TRY(c.dsplit.reserve((size_t)p.mp * p.K * 4));
+    SC_TRY(c.dsplit.reserve((size_t)p.mp * p.K * (G ? 6 : 4)));
     SC_TRY(c.misc.reserve(MISC_BYTES));
     p.d_tc_err = misc_at<int>(c.misc, MISC_TC_ERR);
     SC_CUDA(cudaMemsetAsync(p.d_tc_err, 0, 4, st));
     char* ds = reinterpret_cast<char*>(c.dsplit.ptr);
     pr.mark(ST_GRAM);
-    SC_CUDA(launch_bf16_split(p.dD, p.m, p.m, p.K, p.mp, ds, ds + (size_t)p.mp * p.K * 2, st));
+    const size_t piece = (size_t)p.mp * p.K * 2;
+    SC_CUDA(launch_bf16_split(p.dD, p.m, p.m, p.K, p.mp, ds, ds + piece, st,
+                              G ? ds + 2 * piece : nullptr));
     pr.launches(1);
     p.dDsplit = ds;
     if (G) {
-      SC_CUDA(launch_gram_tc(ds, ds + (size_t)p.mp * p.K * 2, p.mp, p.K, p.Kp, ridge, G,
+      SC_CUDA(launch_gram_tc(ds, ds + piece, ds + 2 * piece, p.mp, p.K, p.Kp, ridge, G,
                              p.d_tc_err, st));
       pr.launches(2);
     }

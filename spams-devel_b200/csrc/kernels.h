@@ -231,8 +231,10 @@ bool tc_gemm_available();
 // rows of the bf16 split operands: m rounded up to the 64-element k-block
 int tc_pad_m(int m);
 // x (rows x cols fp32, ld ldx) -> hi / lo bf16 (rows_pad x cols), zero padded
+// With lo3 set, also the third piece lo3 = bf16(x - hi - lo) (hi + lo + lo3
+// carries FP32's 24 significant bits).
 cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t cols, int rows_pad,
-                              void* hi, void* lo, cudaStream_t st);
+                              void* hi, void* lo, cudaStream_t st, void* lo3 = nullptr);
 // C = sum over the first `nterms` of (Dhi,Xhi), (Dhi,Xlo), (Dlo,Xhi) of
 // D^T X on tcgen05: rows 0..rows_out-1 (rows_out <= K rounded up to 128;
 // rows beyond K come out zero) of each of the n columns (ld ldc).  *err is
@@ -245,9 +247,10 @@ cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* 
 cudaError_t launch_tc_corr_fused(const void* Dhi, const void* Dlo, int K, const float* X,
                                  int64_t ldx, int m, int64_t n, int m_pad, float* C, int ldc,
                                  int rows_out, int* err, cudaStream_t st);
-// G (Kp x Kp) = D^T D + ridge I from the BF16 hi / lo halves of D (m_pad x K
-// each): the 3-term tensor-core product, symmetrised, zero beyond K.
-cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, int Kp, float ridge,
-                           float* G, int* err, cudaStream_t st);
+// G (Kp x Kp) = D^T D + ridge I from the three-piece BF16 split of D
+// (hi, mid = the lo half of the two-piece split, lo3; m_pad x K each): six
+// tensor-core products, FP32-grade, symmetrised, zero beyond K.
+cudaError_t launch_gram_tc(const void* Dhi, const void* Dmid, const void* Dlo3, int m_pad, int K,
+                           int Kp, float ridge, float* G, int* err, cudaStream_t st);
 
 }  // namespace sc

@@ -501,7 +501,7 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
   }
   const size_t gbytes = (size_t)d->Kp * d->Kp * 4;
   const bool tcd = tc_gemm_available();
-  d->bytes = (size_t)m * K * 4 + (tcd ? 4 : 2) * gbytes + (size_t)d->mp * K * 4;
+  d->bytes = (size_t)m * K * 4 + (tcd ? 4 : 2) * gbytes + (size_t)d->mp * K * (tcd ? 6 : 4);
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->reserved_total() + d->bytes > s->budget)
@@ -512,7 +512,7 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
   SC_TRY(d->D.reserve((size_t)m * K * 4));
   SC_TRY(d->Gomp.reserve(gbytes));
   SC_TRY(d->Glasso.reserve(gbytes));
-  SC_TRY(d->split.reserve((size_t)d->mp * K * 4));
+  SC_TRY(d->split.reserve((size_t)d->mp * K * (tcd ? 6 : 4)));  // hi, lo (, lo3 for the Grams)
   SC_CUDA(cudaMemcpyAsync(d->D.ptr, D, (size_t)m * K * 4, cudaMemcpyHostToDevice, st));
   const float* dD = reinterpret_cast<const float*>(d->D.ptr);
   SC_CUDA(launch_gram<float>(dD, m, K, d->Kp, 0.f, reinterpret_cast<float*>(d->Gomp.ptr), st));
@@ -525,10 +525,11 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
     SC_CUDA(cudaMemsetAsync(err, 0, 4, st));
     char* sp = static_cast<char*>(d->split.ptr);
     char* lo = sp + (size_t)d->mp * K * 2;
-    SC_CUDA(launch_bf16_split(dD, m, m, K, d->mp, sp, lo, st));
-    SC_CUDA(launch_gram_tc(sp, lo, d->mp, K, d->Kp, 0.f, reinterpret_cast<float*>(d->GompTc.ptr),
-                           err, st));
-    SC_CUDA(launch_gram_tc(sp, lo, d->mp, K, d->Kp, 1e-10f,
+    char* lo3 = lo + (size_t)d->mp * K * 2;
+    SC_CUDA(launch_bf16_split(dD, m, m, K, d->mp, sp, lo, st, lo3));
+    SC_CUDA(launch_gram_tc(sp, lo, lo3, d->mp, K, d->Kp, 0.f,
+                           reinterpret_cast<float*>(d->GompTc.ptr), err, st));
+    SC_CUDA(launch_gram_tc(sp, lo, lo3, d->mp, K, d->Kp, 1e-10f,
                            reinterpret_cast<float*>(d->GlassoTc.ptr), err, st));
     int herr = 0;
     SC_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));

@@ -106,9 +106,11 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 }
 
 __global__ void __launch_bounds__(128, 1)
-tc_corr_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-               const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-               float* __restrict__ C, int ldc, int rows_out, int64_t n, int m_pad, int nterms,
+tc_corr_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
+               const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
+               const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2,
+               uint32_t term_code, float* __restrict__ C, int ldc, int rows_out, int64_t n,
+               int m_pad, int nterms,
                int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -160,8 +162,10 @@ tc_corr_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ 
       if (*abort_flag || !mbar_wait(empty_bar(s), (round & 1u) ^ 1u)) { *abort_flag = 1; break; }
       const int term = kb / kb_per_term;
       const int kx = (kb % kb_per_term) * TC_BK;
-      const CUtensorMap* ma = term == 2 ? &mAl : &mAh;
-      const CUtensorMap* mb = term == 1 ? &mBl : &mBh;
+      // term t multiplies A piece (code >> 4t) & 3 by B piece (code >> 4t + 2) & 3
+      const uint32_t ia = (term_code >> (4 * term)) & 3u, ib = (term_code >> (4 * term + 2)) & 3u;
+      const CUtensorMap* ma = ia == 0 ? &mA0 : (ia == 1 ? &mA1 : &mA2);
+      const CUtensorMap* mb = ib == 0 ? &mB0 : (ib == 1 ? &mB1 : &mB2);
       uint8_t* st = smem + (size_t)s * TC_STAGE_BYTES;
       mbar_expect_tx(full_bar(s), TC_STAGE_BYTES);
       tma_load_2d(smem_u32(st), ma, full_bar(s), kx, m0);
@@ -485,7 +489,7 @@ tc_corr_fused_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
 // 16-byte loads when the column is 16-byte aligned, two 16-byte stores).
 __global__ void bf16_split_kernel(const float* __restrict__ x, int rows, int64_t ldx, int64_t cols,
                                   int rows_pad, bool vec, __nv_bfloat16* __restrict__ hi,
-                                  __nv_bfloat16* __restrict__ lo) {
+                                  __nv_bfloat16* __restrict__ lo, __nv_bfloat16* __restrict__ lo3) {
   const int groups = rows_pad >> 3;
   const int64_t total = cols * groups;
   for (int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gid < total;
@@ -503,15 +507,18 @@ __global__ void bf16_split_kernel(const float* __restrict__ x, int rows, int64_t
 #pragma unroll
       for (int k = 0; k < 8; ++k) v[k] = r0 + k < rows ? src[k] : 0.f;
     }
-    __align__(16) __nv_bfloat16 h[8], l[8];
+    __align__(16) __nv_bfloat16 h[8], l[8], l3[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       h[k] = __float2bfloat16_rn(v[k]);
-      l[k] = __float2bfloat16_rn(v[k] - __bfloat162float(h[k]));
+      const float r = v[k] - __bfloat162float(h[k]);
+      l[k] = __float2bfloat16_rn(r);
+      l3[k] = __float2bfloat16_rn(r - __bfloat162float(l[k]));
     }
     const size_t o = (size_t)c * rows_pad + r0;
     *reinterpret_cast<uint4*>(hi + o) = *reinterpret_cast<const uint4*>(h);
     *reinterpret_cast<uint4*>(lo + o) = *reinterpret_cast<const uint4*>(l);
+    if (lo3) *reinterpret_cast<uint4*>(lo3 + o) = *reinterpret_cast<const uint4*>(l3);
   }
 }
 
@@ -552,8 +559,9 @@ bool tc_gemm_available() { return load_encode(); }
 int tc_pad_m(int m) { return ((m + TC_BK - 1) / TC_BK) * TC_BK; }
 
 cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t cols, int rows_pad,
-                              void* hi, void* lo, cudaStream_t st) {
-  if (rows_pad % 8 != 0 || ((uintptr_t)hi & 15u) || ((uintptr_t)lo & 15u))
+                              void* hi, void* lo, cudaStream_t st, void* lo3) {
+  if (rows_pad % 8 != 0 || ((uintptr_t)hi & 15u) || ((uintptr_t)lo & 15u) ||
+      ((uintptr_t)lo3 & 15u))
     return cudaErrorInvalidValue;
   const int64_t tot = (int64_t)(rows_pad / 8) * cols;
   if (tot <= 0) return cudaSuccess;
@@ -561,7 +569,8 @@ cudaError_t launch_bf16_split(const float* x, int rows, int64_t ldx, int64_t col
   const int64_t blocks = std::min<int64_t>((tot + 255) / 256, (int64_t)148 * 32);
   bf16_split_kernel<<<(unsigned)blocks, 256, 0, st>>>(x, rows, ldx, cols, rows_pad, vec,
                                                       reinterpret_cast<__nv_bfloat16*>(hi),
-                                                      reinterpret_cast<__nv_bfloat16*>(lo));
+                                                      reinterpret_cast<__nv_bfloat16*>(lo),
+                                                      reinterpret_cast<__nv_bfloat16*>(lo3));
   return cudaGetLastError();
 }
 
@@ -589,18 +598,40 @@ cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* 
                                        (int)TC_SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid(Kp / TC_BM, (unsigned)gy);
-  tc_corr_kernel<<<grid, 128, TC_SMEM, st>>>(mAh, mAl, mBh, mBl, C, ldc, rows_out, n, m_pad,
-                                              nterms, err);
+  // terms (hi, hi), (hi, lo), (lo, hi): pieces (A, B) = (0, 0), (0, 1), (1, 0)
+  const uint32_t code = 0u | (4u << 4) | (1u << 8);
+  tc_corr_kernel<<<grid, 128, TC_SMEM, st>>>(mAh, mAl, mAl, mBh, mBl, mBl, code, C, ldc, rows_out,
+                                              n, m_pad, nterms, err);
   return cudaGetLastError();
 }
 
-// G = D^T D (+ ridge on the diagonal) from the BF16 hi / lo halves of D:
-// the correlation product with X = D (3 terms, FP32 accumulation), whose
-// upper triangle is then mirrored (as Matrix::fillSymmetric does after syrk)
-// and whose padding rows / columns are zeroed.  Two launches.
-cudaError_t launch_gram_tc(const void* Dhi, const void* Dlo, int m_pad, int K, int Kp, float ridge,
-                           float* G, int* err, cudaStream_t st) {
-  cudaError_t e = launch_tc_corr(Dhi, Dlo, K, Dhi, Dlo, K, m_pad, 3, G, Kp, Kp, err, st);
+// G = D^T D (+ ridge on the diagonal) from a three-piece BF16 split of D
+// (d = hi + mid + lo, 24 significant bits as in FP32): the six products
+// hi hi, hi mid, mid hi, hi lo, lo hi, mid mid with FP32 accumulation on the
+// tensor cores (the three dropped ones are below FP32 rounding), then the
+// upper triangle mirrored (as Matrix::fillSymmetric does after syrk) and
+// the padding rows / columns zeroed.  A two-piece split would leave the Gram
+// at ~16 bits, which OMP's unit-norm bookkeeping amplifies where an atom's
+// residual norm is small.  Two launches.
+cudaError_t launch_gram_tc(const void* Dhi, const void* Dmid, const void* Dlo3, int m_pad, int K,
+                           int Kp, float ridge, float* G, int* err, cudaStream_t st) {
+  if (K <= 0) return cudaSuccess;
+  if (!load_encode()) return cudaErrorNotSupported;
+  if (m_pad % TC_BK != 0 || Kp < ((K + TC_BM - 1) / TC_BM) * TC_BM) return cudaErrorInvalidValue;
+  CUtensorMap m0, m1, m2;
+  if (!make_map(&m0, Dhi, m_pad, K, TC_BM) || !make_map(&m1, Dmid, m_pad, K, TC_BM) ||
+      !make_map(&m2, Dlo3, m_pad, K, TC_BM))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(tc_corr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TC_SMEM);
+  if (e != cudaSuccess) return e;
+  const int kt = (K + TC_BM - 1) / TC_BM;
+  dim3 grid(kt, kt);
+  // (A, B) pieces per term: (0,0) (0,1) (1,0) (0,2) (2,0) (1,1)
+  const uint32_t code = 0u | (4u << 4) | (1u << 8) | (8u << 12) | (2u << 16) | (5u << 20);
+  tc_corr_kernel<<<grid, 128, TC_SMEM, st>>>(m0, m1, m2, m0, m1, m2, code, G, Kp, kt * TC_BM,
+                                              (int64_t)K, m_pad, 6, err);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return launch_symmetrize<float>(G, K, Kp, ridge, st);
 }

@@ -140,6 +140,10 @@ def lib() -> C.CDLL:
                                     f32p, opt, C.POINTER(CscF32)]),
         "sc_lasso_gram_f64": (i32, [f64p, i32, i64, f64p, i32, f64p, i32, d, d, i32, i32, i32, i32,
                                     f64p, opt, C.POINTER(CscF64)]),
+        "sc_lasso_gram_chol_f32": (i32, [f32p, i32, i64, f32p, i32, f32p, i32, f, f, i32, i32,
+                                         i32, i32, i32, i32, f32p, opt, C.POINTER(CscF32)]),
+        "sc_lasso_gram_chol_f64": (i32, [f64p, i32, i64, f64p, i32, f64p, i32, d, d, i32, i32,
+                                         i32, i32, i32, i32, f64p, opt, C.POINTER(CscF64)]),
         "sc_omp_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, p, p, p, p, p, p, i64, i64p, p,
                                  opt]),
         "sc_lasso_f32_dev": (i32, [p, i32, i64, p, i32, i32, f, f, i32, i32, i32, p, p, p, i64,
@@ -168,6 +172,9 @@ def lib() -> C.CDLL:
         "sc_lasso_mask_f64": (i32, [f64p, i32, i64, f64p, i32, C.POINTER(C.c_uint8), i32, d, d, i32, i32, i32,
                                     opt, C.POINTER(CscF64)]),
     }
+    missing = sorted(set(EXPORTS) - set(sigs))
+    if missing:  # every exported entry point is called with a declared signature
+        raise ImportError(f"spams_b200: no ctypes signature for {missing}")
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
         fn.restype = res

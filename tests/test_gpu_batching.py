@@ -9,7 +9,7 @@ import spams_b200
 from spams_b200 import workloads as W
 from oracle import oracle as O
 
-from conftest import rel_err, support_match
+from conftest import matched_columns, rel_err, support_match
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -66,4 +66,4 @@ def test_graph_replay_of_uneven_omp_matches_eager_call(prec):
                         L=Lv[:ns].cpu().numpy(), eps=eps[:ns].double().cpu().numpy())
         a = eager[:, :ns]
         assert support_match(a, ref) >= 0.995
-        assert rel_err(a, ref) <= 1e-4
+        assert rel_err(*matched_columns(a, ref)) <= 1e-4
