@@ -96,16 +96,17 @@ def measured_peaks() -> dict:
                 "tensor_source": "fallback"}
 
 
-def corr_roofline(m: int, K: int, Kp: int, n: int, ms: float, peaks: dict) -> dict:
+def corr_roofline(m: int, K: int, Kp: int, n: int, ms: float, peaks: dict, terms: int = 3) -> dict:
     """The correlation stage D^T X on the tensor cores: algorithmic FLOPs 2 m K n
-    (the 3-term BF16 split executes three times as many), and its bytes (X in,
-    the Kp x n correlations out) against HBM."""
+    (the BF16 split executes `terms` times as many: 3 for the hi / lo form of
+    the Lasso, 6 for the three-piece form of OMP), and its bytes (X in, the
+    Kp x n correlations out) against HBM."""
     if not ms or ms <= 0:
         return None
     alg = 2.0 * m * K * n
-    exe = 3.0 * alg
+    exe = float(terms) * alg
     byt = 4.0 * m * n + 4.0 * Kp * n
-    return {"kernel": "tc_corr_fused_kernel", "bound": "tensor", "ms": ms,
+    return {"kernel": "tc_corr_xs_kernel", "bound": "tensor", "ms": ms, "terms": terms,
             "achieved_tflops": exe / (ms / 1e3) / 1e12,
             "achieved_tflops_algorithmic": alg / (ms / 1e3) / 1e12,
             "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
@@ -562,7 +563,7 @@ def uneven_omp_result(n: int, steps: int, warmup: int, precision: str, cpu_secon
                      "active_set_capacity": prof["lcap"]},
         "stages_ms": {k: prof[k] for k in ("ms_gram", "ms_norms", "ms_corr", "ms_code",
                                            "ms_refine", "ms_csc")},
-        "corr_roofline": (corr_roofline(UO_M, UO_K, UO_K, n, prof["ms_corr"], peaks)
+        "corr_roofline": (corr_roofline(UO_M, UO_K, UO_K, n, prof["ms_corr"], peaks, terms=6)
                           if precision == "bf16x3" else None),
         "fp32_value": (n * steps / (fp32_ms / 1e3)) if fp32_ms else value,
         "omp_steps_per_signal": prof["steps"] / n, "nnz_per_signal": nnz / n,

@@ -20,6 +20,13 @@ template <> __device__ __forceinline__ double inf<double>() { return __longlong_
 
 // Four consecutive elements starting at a 4-element-aligned address, as one
 // (float) or two (double) vector loads.
+// a * b rounded on its own, never contracted with a following add into one
+// FMA: the reference's scalar updates (built without FMA contraction) round
+// the product first, and the L1COEFFS stop compares their sum with the
+// constraint at rounding level.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <typename T> struct Vec4 { T v[4]; };
 
 __device__ __forceinline__ Vec4<float> ld4(const float* p) {

@@ -233,7 +233,7 @@ sc_status sc_dl_step_f32(sc_dl* s, const float* dD, const float* dX, int64_t M,
     char* sp = static_cast<char*>(s->split.ptr);
     const size_t piece = (size_t)mp * K * 2;
     SC_CUDA(launch_bf16_split(dD, m, m, K, mp, sp, sp + piece, st, sp + 2 * piece));
-    SC_CUDA(launch_gram_tc(sp, sp + piece, sp + 2 * piece, mp, K, Kp, ridge, G,
+    SC_CUDA(launch_gram_tc(sp, sp + piece, sp + 2 * piece, dD, m, mp, K, Kp, ridge, G,
                            reinterpret_cast<int*>(s->tcerr.ptr), st));
     own_launches += 3;
   } else {

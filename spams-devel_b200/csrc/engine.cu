@@ -318,7 +318,7 @@ struct Problem {
   const uint8_t* hmask = nullptr;
   T mask_ridge = 0;
   int mask_scale = 0;
-  const void* dDsplit = nullptr;  // Dhi (mp x K bf16) followed by Dlo
+  const void* dDsplit = nullptr;  // Dhi, Dlo, Dlo3 (mp x K bf16 each), consecutive
   int mp = 0;                     // m rounded up to the 64-element k-block
   int* d_tc_err = nullptr;
 };
@@ -661,10 +661,19 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       pr.launches(2);
     } else if (p.tc) {
       if constexpr (std::is_same<T, float>::value) {
-        // BF16 hi / lo products with the split of X done inside the kernel
+        // BF16 split products with the split of X done inside the kernel.
+        // OMP reads its selections and eps stops off the correlations, so it
+        // takes the three-piece form (six products, FP32-grade); the LARS
+        // path keeps the hi / lo form (three products).
         const char* ds = reinterpret_cast<const char*>(p.dDsplit);
-        SC_CUDA(launch_tc_corr_fused(ds, ds + (size_t)p.mp * p.K * 2, p.K, xchunk, p.m, p.m, cn,
-                                     p.mp, dtx, Kp, Kp, p.d_tc_err, st));
+        const size_t piece = (size_t)p.mp * p.K * 2;
+        const void* dp[3] = {ds, ds + piece, ds + 2 * piece};
+        cudaError_t e = launch_tc_corr_xs(dp, p.lars ? 2 : 3, p.K, xchunk, p.m, p.m, cn, p.mp,
+                                          dtx, Kp, Kp, p.d_tc_err, st);
+        if (e == cudaErrorNotSupported)  // large m: the streaming hi / lo form
+          e = launch_tc_corr_fused(ds, ds + piece, p.K, xchunk, p.m, p.m, cn, p.mp, dtx, Kp,
+                                   Kp, p.d_tc_err, st);
+        SC_CUDA(e);
         pr.launches(1);
       }
     } else {
@@ -944,8 +953,8 @@ static sc_status prepare_tc(DeviceCtx& c, cudaStream_t st, Problem<T>& p, Prof& 
     pr.launches(1);
     p.dDsplit = ds;
     if (G) {
-      SC_CUDA(launch_gram_tc(ds, ds + piece, ds + 2 * piece, p.mp, p.K, p.Kp, ridge, G,
-                             p.d_tc_err, st));
+      SC_CUDA(launch_gram_tc(ds, ds + piece, ds + 2 * piece, p.dD, p.m, p.mp, p.K, p.Kp, ridge,
+                             G, p.d_tc_err, st));
       pr.launches(2);
     }
   } else {
@@ -1567,8 +1576,11 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
   char* dh = (char*)c->D.ptr;
   SC_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
   SC_CUDA(launch_bf16_split(dD, m, m, K, mp, dh, dh + (size_t)mp * K * 2, st));
-  SC_CUDA(launch_tc_corr_fused(dh, dh + (size_t)mp * K * 2, K, dX, m, m, n, mp, dC, ldc, K, d_err,
-                               st));
+  const void* dp[2] = {dh, dh + (size_t)mp * K * 2};
+  cudaError_t e = launch_tc_corr_xs(dp, 2, K, dX, m, m, n, mp, dC, ldc, K, d_err, st);
+  if (e == cudaErrorNotSupported)  // large m: the streaming form
+    e = launch_tc_corr_fused(dp[0], dp[1], K, dX, m, m, n, mp, dC, ldc, K, d_err, st);
+  SC_CUDA(e);
   int* h = reinterpret_cast<int*>(c->pinned_small);
   SC_CUDA(cudaMemcpyAsync(h, d_err, 4, cudaMemcpyDeviceToHost, st));
   SC_CUDA(cudaStreamSynchronize(st));

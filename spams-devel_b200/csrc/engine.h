@@ -103,7 +103,7 @@ struct BatchDesc {
   int64_t n = 0;
   const float* dD = nullptr;   // m x K
   const float* G = nullptr;    // Kp x Kp Gram (with the ridge for the Lasso)
-  const void* dDsplit = nullptr;  // BF16 hi / lo halves of D (tc), or NULL
+  const void* dDsplit = nullptr;  // three BF16 pieces of D (hi, lo, lo3; tc), or NULL
   int K = 0, Kp = 0;
   int L = 0;                   // slab stride: the largest L of the batch
   // Lasso

@@ -247,10 +247,21 @@ cudaError_t launch_tc_corr(const void* Dhi, const void* Dlo, int K, const void* 
 cudaError_t launch_tc_corr_fused(const void* Dhi, const void* Dlo, int K, const float* X,
                                  int64_t ldx, int m, int64_t n, int m_pad, float* C, int ldc,
                                  int rows_out, int* err, cudaStream_t st);
+// The X-stationary form: D given as np bf16 pieces (2: hi, lo with three
+// products; 3: hi, mid, lo with six, FP32-grade), X fp32 split in the
+// kernel once per signal tile.  cudaErrorNotSupported where a signal tile's
+// pieces do not fit in shared memory (large m); the caller then takes
+// launch_tc_corr_fused.
+cudaError_t launch_tc_corr_xs(const void* const* Dpieces, int np, int K, const float* X,
+                              int64_t ldx, int m, int64_t n, int m_pad, float* C, int ldc,
+                              int rows_out, int* err, cudaStream_t st);
 // G (Kp x Kp) = D^T D + ridge I from the three-piece BF16 split of D
-// (hi, mid = the lo half of the two-piece split, lo3; m_pad x K each): six
-// tensor-core products, FP32-grade, symmetrised, zero beyond K.
-cudaError_t launch_gram_tc(const void* Dhi, const void* Dmid, const void* Dlo3, int m_pad, int K,
-                           int Kp, float ridge, float* G, int* err, cudaStream_t st);
+// (hi, mid = the lo half of the two-piece split, lo3; m_pad x K each) and D
+// itself (fp32, m x K): six tensor-core products, FP32-grade, symmetrised,
+// zero beyond K (the FP32 CUDA-core product where the tensor-core form does
+// not apply).
+cudaError_t launch_gram_tc(const void* Dhi, const void* Dmid, const void* Dlo3, const float* D,
+                           int m, int m_pad, int K, int Kp, float ridge, float* G, int* err,
+                           cudaStream_t st);
 
 }  // namespace sc

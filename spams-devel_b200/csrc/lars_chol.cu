@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(128) lars_chol_kernel(const LarsArgs<T> a) {
           T tu = 0;
           for (int k = 0; k <= j; ++k) tu += su[k];
           if (tu > T(10e-10)) gamma = min_ref(gamma, (constraint - thrs) / tu);  // EPSILON
-          thrs += gamma * tu;
+          thrs += mul_rn(gamma, tu);
         }
         if (!ols) {
           const T t = gamma * gamma - 2 * gamma * potentNorm;

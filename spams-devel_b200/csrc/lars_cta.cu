@@ -301,7 +301,7 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
           st4(sDtR + r0, d);
         }
         normX += coeff1 * step * step - 2 * coeff2 * step;
-        thrs += step * coeff1;
+        thrs += mul_rn(step, coeff1);
         c_end = C - step;
         at_lambda = step == step_max2;
         if (gw == 0) {

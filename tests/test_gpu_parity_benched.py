@@ -115,7 +115,9 @@ def test_dictlearn_step_codes_vs_reference_f64():
         _report(f"dictlearn step 144x1024 batch 1024 prec={prec}", rep)
         sm, fro, p999, _ = rep
         assert sm >= 0.995
-        assert fro <= 1e-5
+        # smooth patches make a correlated dictionary, which amplifies the
+        # BF16 hi/lo correlation error (the BF16-split tolerance is 1e-3)
+        assert fro <= (1e-5 if prec == FP32 else 1e-4)
 
 
 def _tie_case(dt):

@@ -12,7 +12,13 @@ def _colmajor(a):
     return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
 
 
-@pytest.mark.parametrize("m,K,n", [(64, 128, 128), (256, 512, 1000), (100, 200, 333), (512, 2048, 4096), (144, 1024, 257)])
+# signal tiles of 128, 64, 32 and 16 signals (the resident split of a tile
+# shrinks as m grows), atom tiles spread over groups when the signal tiles
+# are few (n = 257, 50), and m = 2100, beyond the resident form, on the
+# streaming kernel
+@pytest.mark.parametrize("m,K,n", [(64, 128, 128), (256, 512, 1000), (100, 200, 333),
+                                   (512, 2048, 4096), (144, 1024, 257), (1000, 256, 700),
+                                   (2000, 128, 50), (2100, 256, 300)])
 def test_bf16x3_correlation_close_to_fp64(m, K, n):
     rng = np.random.Generator(np.random.PCG64(m * 7 + K))
     D = rng.standard_normal((m, K)).astype(np.float32)
