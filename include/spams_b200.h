@@ -12,8 +12,10 @@
  *
  * Host vs device pointers:
  *   sc_omp_* / sc_lasso_* / sc_lasso_gram_* take HOST arrays and return a CSC
- *   matrix in malloc'd host arrays (free with sc_csc_free).  They copy the
- *   inputs to the device, run, and copy the result back (blocking).
+ *   matrix in host arrays owned by the library (page-locked blocks from a
+ *   reused pool where possible, else malloc'd; free them with sc_csc_free,
+ *   never with free()).  They copy the inputs to the device, run, and copy
+ *   the result back (blocking).
  *   sc_*_dev variants take DEVICE arrays, write the CSC into caller-provided
  *   device arrays and run asynchronously on the given CUDA stream.
  *

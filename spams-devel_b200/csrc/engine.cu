@@ -323,8 +323,88 @@ struct Problem {
   int* d_tc_err = nullptr;
 };
 
-// CSC result assembled on the host: malloc'd arrays whose ownership moves to
-// the caller's sc_csc_* (freed by sc_csc_free_*).
+// Host result arrays: page-locked blocks from a process-wide pool, so that
+// the read-back of each chunk's CSC is a DMA straight into the result at
+// full link speed, runs asynchronously, and touches no fresh pages (a
+// malloc'd result is pageable: its copies are staged and synchronous, and its
+// first touch faults every page in).  Blocks go back to the pool when the
+// caller frees the result (sc_csc_free_*); past kResultPoolBytes of pinned
+// memory, or when page-locking fails, results fall back to malloc.
+constexpr size_t kResultPoolBytes = (size_t)1 << 30;
+struct ResultPool {
+  std::mutex mu;
+  std::map<void*, std::pair<size_t, bool>> blocks;  // base -> (bytes, in use)
+  size_t total = 0;
+};
+static ResultPool& result_pool() {
+  static ResultPool* p = new ResultPool();  // outlives every caller's result
+  return *p;
+}
+// A block of at least `bytes` (pinned when possible), or NULL.
+static void* result_alloc(size_t bytes) {
+  if (bytes == 0) bytes = 1;
+  ResultPool& rp = result_pool();
+  {
+    std::lock_guard<std::mutex> lk(rp.mu);
+    void* best = nullptr;
+    size_t best_size = 0;
+    for (auto& kv : rp.blocks)  // smallest free block that fits, at most 4x too large
+      if (!kv.second.second && kv.second.first >= bytes && kv.second.first <= 4 * bytes &&
+          (!best || kv.second.first < best_size)) {
+        best = kv.first;
+        best_size = kv.second.first;
+      }
+    if (best) {
+      rp.blocks[best].second = true;
+      return best;
+    }
+  }
+  size_t sz = 4096;
+  while (sz < bytes) sz <<= 1;  // power-of-two sizes, so that blocks are reused
+  void* p = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(rp.mu);
+    if (rp.total + sz <= kResultPoolBytes &&
+        cudaHostAlloc(&p, sz, cudaHostAllocPortable) == cudaSuccess) {
+      rp.blocks[p] = {sz, true};
+      rp.total += sz;
+      return p;
+    }
+  }
+  (void)cudaGetLastError();  // a refused page-lock is not a sticky error
+  return malloc(bytes);
+}
+// Frees a result array from result_alloc (or malloc).
+static void result_free(void* p) {
+  if (!p) return;
+  ResultPool& rp = result_pool();
+  {
+    std::lock_guard<std::mutex> lk(rp.mu);
+    auto it = rp.blocks.find(p);
+    if (it != rp.blocks.end()) {
+      it->second.second = false;
+      return;
+    }
+  }
+  free(p);
+}
+// Returns the pool's free blocks to the system (sc_release_all).
+static void result_pool_trim() {
+  ResultPool& rp = result_pool();
+  std::lock_guard<std::mutex> lk(rp.mu);
+  for (auto it = rp.blocks.begin(); it != rp.blocks.end();) {
+    if (!it->second.second) {
+      cudaFreeHost(it->first);
+      rp.total -= it->second.first;
+      it = rp.blocks.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// CSC result assembled on the host in result_alloc blocks, whose ownership
+// moves to the caller's sc_csc_* (freed by sc_csc_free_*).
 template <typename T>
 struct HostSink {
   int64_t* colptr = nullptr;
@@ -334,34 +414,44 @@ struct HostSink {
   HostSink() = default;
   HostSink(const HostSink&) = delete;
   HostSink& operator=(const HostSink&) = delete;
-  ~HostSink() { free(colptr); free(rows); free(vals); }
+  ~HostSink() { result_free(colptr); result_free(rows); result_free(vals); }
   sc_status init(int64_t n) {
-    colptr = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
-    if (!colptr) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
+    colptr = (int64_t*)result_alloc(((size_t)n + 1) * sizeof(int64_t));
+    if (!colptr) return fail(SC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    memset(colptr, 0, ((size_t)n + 1) * sizeof(int64_t));
     return SC_OK;
+  }
+  // Moves the first nnz entries into blocks of `want` entries; false (and no
+  // change) when an allocation fails.  No copy into the old blocks may be in
+  // flight.
+  bool resize(size_t want) {
+    int32_t* r = (int32_t*)result_alloc(want * sizeof(int32_t));
+    T* v = (T*)result_alloc(want * sizeof(T));
+    if (!r || !v) {
+      result_free(r);
+      result_free(v);
+      return false;
+    }
+    if (nnz) {
+      memcpy(r, rows, nnz * sizeof(int32_t));
+      memcpy(v, vals, nnz * sizeof(T));
+    }
+    result_free(rows);
+    result_free(vals);
+    rows = r;
+    vals = v;
+    cap = want;
+    return true;
   }
   // Best-effort capacity for `want` entries (a failed allocation is left to
   // grow()).
   void hint(size_t want) {
-    if (want <= cap) return;
-    int32_t* r = (int32_t*)realloc(rows, want * sizeof(int32_t));
-    if (!r) return;
-    rows = r;
-    T* v = (T*)realloc(vals, want * sizeof(T));
-    if (!v) return;  // rows keeps its larger block; cap still describes vals
-    vals = v;
-    cap = want;
+    if (want > cap) (void)resize(want);
   }
   sc_status grow(size_t need) {
     if (need <= cap) return SC_OK;
-    size_t c2 = std::max(need, cap + cap / 2);
-    int32_t* r = (int32_t*)realloc(rows, c2 * sizeof(int32_t));
-    if (!r) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
-    rows = r;
-    T* v = (T*)realloc(vals, c2 * sizeof(T));
-    if (!v) return fail(SC_ERR_OUT_OF_MEMORY, "host malloc failed");
-    vals = v;
-    cap = c2;
+    if (!resize(std::max(need, cap + cap / 2)))
+      return fail(SC_ERR_OUT_OF_MEMORY, "host allocation failed");
     return SC_OK;
   }
 };
@@ -521,6 +611,15 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // chunk i's CSC: its column pointers were read back into pinned memory on
   // the coding stream; the entries are copied straight into the result
   int64_t nnz_total = 0;
+  bool d2h_pending[2] = {false, false};  // an entry read-back per slot still in flight
+  struct D2hDrain {  // no read-back outlives the call, whatever its exit
+    DeviceCtx& c;
+    bool* pending;
+    ~D2hDrain() {
+      for (int k = 0; k < 2; ++k)
+        if (pending[k]) cudaEventSynchronize(c.ev_d2h[k]);
+    }
+  } d2h_guard{c, d2h_pending};
   auto finalize = [&](int64_t i) -> sc_status {
     const int64_t cn = chunk_len(i);
     const int slot = piped ? (int)(i & 1) : 0;
@@ -528,9 +627,28 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     const int64_t* hcol =
         reinterpret_cast<const int64_t*>(static_cast<char*>(c.pinned_col) + slot * col_slot);
     const int64_t cnnz = hcol[cn];
-    if (i == 0 && p.n > cn)  // the whole result at the first chunk's density, +15%
+    // entry copies still in flight must land before the result blocks move
+    // (a resize), and before the device slot they read is refilled (the
+    // chunk after next waits on the host for this finalize)
+    auto drain = [&]() -> sc_status {
+      for (int k = 0; k < 2; ++k)
+        if (d2h_pending[k]) {
+          SC_CUDA(cudaEventSynchronize(c.ev_d2h[k]));
+          d2h_pending[k] = false;
+        }
+      return SC_OK;
+    };
+    const size_t need = (size_t)(nnz_total + cnnz);
+    if (i == 0 && p.n > cn) {  // the whole result at the first chunk's density, +15%
+      SC_TRY(drain());
       sink->hint((size_t)((double)cnnz * (double)p.n / (double)cn * 1.15) + 1024);
-    SC_TRY(sink->grow((size_t)(nnz_total + cnnz)));
+    }
+    if (need > sink->cap) SC_TRY(drain());
+    SC_TRY(sink->grow(need));
+    if (d2h_pending[slot]) {
+      SC_CUDA(cudaEventSynchronize(c.ev_d2h[slot]));
+      d2h_pending[slot] = false;
+    }
     if (cnnz > 0) {
       cudaStream_t cs = piped ? c.d2h_stream : st;
       SC_CUDA(cudaMemcpyAsync(sink->rows + nnz_total,
@@ -540,7 +658,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
                               static_cast<char*>(c.cvals.ptr) + slot * align16(ent_slot * sizeof(T)),
                               (size_t)cnnz * sizeof(T), cudaMemcpyDeviceToHost, cs));
       SC_CUDA(cudaEventRecord(c.ev_d2h[slot], cs));
-      SC_CUDA(cudaEventSynchronize(c.ev_d2h[slot]));
+      d2h_pending[slot] = true;
+      if (!piped || i + 1 == nchunks) SC_TRY(drain());
     }
     int64_t* dst = sink->colptr + chunk_start(i);
     for (int64_t k = 0; k <= cn; ++k) dst[k] = nnz_total + hcol[k];
@@ -794,13 +913,16 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     int64_t* scratch = reinterpret_cast<int64_t*>(W.scan.ptr);
     if (sink) {
       const int slot = piped ? (int)(ci & 1) : 0;
-      // the read-back of the chunk that used these slots before has ended
-      // (finalize waits for it on the host)
+      // the column pointers of the chunk that used these slots before were
+      // read on the host (finalize); its entries' read-back is waited for
+      // on the device below
       int64_t* ccol = reinterpret_cast<int64_t*>(static_cast<char*>(c.ccolptr.ptr) + slot * col_slot);
       int32_t* crow = reinterpret_cast<int32_t*>(static_cast<char*>(c.crows.ptr) +
                                                  slot * align16(ent_slot * 4));
       T* cval = reinterpret_cast<T*>(static_cast<char*>(c.cvals.ptr) +
                                      slot * align16(ent_slot * sizeof(T)));
+      // the read-back of the chunk that last used this slot's entries ends first
+      if (d2h_pending[slot]) SC_CUDA(cudaStreamWaitEvent(st, c.ev_d2h[slot], 0));
       SC_CUDA(launch_scan_counts(cnt, cn, ccol, nullptr, scratch, scan_len, st));
       SC_CUDA(launch_csc_gather<T>(sind, sval, p.L, cnt, ccol, cn, nullptr, cn * (int64_t)p.L,
                                    d_capflag, crow, cval, st));
@@ -1400,15 +1522,18 @@ sc_status sc_device_count(int* count) {
 
 void sc_csc_free_f32(sc_csc_f32* a) {
   if (!a) return;
-  free(a->colptr); free(a->rows); free(a->vals);
+  sc::result_free(a->colptr); sc::result_free(a->rows); sc::result_free(a->vals);
   memset(a, 0, sizeof(*a));
 }
 void sc_csc_free_f64(sc_csc_f64* a) {
   if (!a) return;
-  free(a->colptr); free(a->rows); free(a->vals);
+  sc::result_free(a->colptr); sc::result_free(a->rows); sc::result_free(a->vals);
   memset(a, 0, sizeof(*a));
 }
-void sc_release_all(void) { sc::release_all(); }
+void sc_release_all(void) {
+  sc::release_all();
+  sc::result_pool_trim();
+}
 
 sc_status sc_last_profile(sc_profile* out) {
   if (!out) return fail(SC_ERR_INVALID_ARG, "null profile");

@@ -118,9 +118,9 @@ inline int pick_fastest(const std::vector<float>& t, float margin = kTuneMargin)
 // (at least kPipeMinChunk signals) after a first chunk half that size: while
 // one chunk is coded, the next one is copied in on the H2D stream and the
 // previous chunk's CSC is read back.  Measured on the 100k-signal lasso
-// workload: 3.31 ms end to end against 3.36 with a quarter-size first chunk,
-// 3.30-3.94 ms for 3 to 8 chunks; a second coding stream for alternate chunks
-// was slower.
+// workload, with page-locked results (the H2D of its 102 MB alone takes
+// 1.85 ms): 2.77 ms end to end; 2.83 with a quarter-size first chunk, 2.88
+// with 8 chunks, 3.17 with 10 (more chunks, more persistent-grid tails).
 constexpr int kPipeChunks = 5;
 constexpr int64_t kPipeMinChunk = 16384;
 constexpr int64_t kPipeFirstDiv = 2;
