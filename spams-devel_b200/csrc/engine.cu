@@ -989,14 +989,14 @@ static sc_status emit_sink(int64_t m, int64_t n, HostSink<T>& s, typename CscOf<
 
 static inline int pad128(int K) { return ((K + 127) / 128) * 128; }
 // Padded atom count: a multiple of 128 up to 1024 atoms (one warp per signal),
-// of 512 beyond (one CTA of Kp / 512 warps per signal).
+// beyond that the CTA kernels' layout (one CTA of Kp / 512 warps per signal).
 int pad_atoms(int K) {
   const int p = pad128(K);
-  return p <= kWarpMaxKp ? p : ((K + 511) / 512) * 512;
+  return p <= kWarpMaxKp ? p : cta_pad_atoms(K);
 }
-// The layout for a forced kernel family: CTA kernels need Kp % 512 == 0.
+// The layout for a forced kernel family: the CTA kernels' own.
 static int pad_atoms_for(int K, const sc_options* opt) {
-  return opt && opt->kernel == SC_KERNEL_CTA ? ((K + 511) / 512) * 512 : pad_atoms(K);
+  return opt && opt->kernel == SC_KERNEL_CTA ? cta_pad_atoms(K) : pad_atoms(K);
 }
 // The masked variants run on the warp-per-signal kernels only.
 static sc_status check_mask(int K, const uint8_t* mask, const sc_options* opt) {
@@ -1107,6 +1107,19 @@ sc_status check_atoms(int K) {
                 kCtaMaxKp, K);
   return SC_OK;
 }
+// OMP keeps two K-vectors per signal in shared memory (residual correlations
+// and atom norms): in double precision that is 256 KB at 16384 atoms, past
+// the 227 KB a block may use, so double-precision OMP stops at 12288.
+template <typename T>
+static sc_status check_omp_atoms(int K) {
+  SC_TRY(check_atoms(K));
+  constexpr int kOmpF64MaxKp = 12288;
+  if (sizeof(T) == 8 && pad_atoms(K) > kOmpF64MaxKp)
+    return fail(SC_ERR_UNSUPPORTED,
+                "double-precision omp takes at most %d atoms (K=%d; single precision: %d)",
+                kOmpF64MaxKp, K, kCtaMaxKp);
+  return SC_OK;
+}
 
 // ---------------------------------------------------------------------------
 // OMP (host arrays)
@@ -1141,7 +1154,7 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (L <= 0) return emit_empty<T>(0, 0, out);  // spalpha.clear(); return
   L = std::min(m, std::min(L, K));
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
-  SC_TRY(check_atoms(K));
+  SC_TRY(check_omp_atoms<T>(K));
   SC_TRY(check_mask(K, mask, opt));
 
   SC_TRY(check_opts<T>(opt));
@@ -1405,7 +1418,7 @@ static sc_status omp_dev(const T* dX, int m, int64_t n, const T* dD, int K, int 
   if (m <= 0 || n < 0 || K <= 0) return fail(SC_ERR_INVALID_ARG, "omp : bad dimensions");
   if (!dX || !dD || !d_colptr || (cap > 0 && (!d_rows || !d_vals)))
     return fail(SC_ERR_INVALID_ARG, "omp : null device pointer");
-  SC_TRY(check_atoms(K));
+  SC_TRY(check_omp_atoms<T>(K));
   SC_TRY(check_opts<T>(opt));
   SC_TRY(check_kernel(K, opt));
   DeviceCtx* c = nullptr;

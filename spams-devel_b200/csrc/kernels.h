@@ -120,7 +120,8 @@ cudaError_t launch_lars(const LarsArgs<T>& a, int grid, int warps_per_block, cud
 template <typename T>
 int lars_max_warps_per_sm(int Kp);
 
-// One CTA of Kp / 512 warps per signal (Kp a multiple of 512, 512..4096);
+// One CTA of Kp / 512 warps per signal (Kp a multiple of 512: 512..4096, 6144,
+// 8192, 12288 or 16384);
 // a.gstate set: per-CTA small state in global slabs (lars_cta_gstate_bytes).
 // grid <= 0: as many persistent blocks as fit on the device.
 template <typename T>

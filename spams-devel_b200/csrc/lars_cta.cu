@@ -8,7 +8,8 @@
 // candidates, the correlation update) runs on all warps; cross-warp
 // arg-minima go through a W-entry exchange.  Every thread derives the step
 // and the control flow from the same shared values, so they agree bitwise.
-// Used for Kp = 512 .. 4096 (W = Kp / 512) and active-set capacities up to L.
+// Used for Kp = 512 .. 4096 and 6144, 8192, 12288, 16384 (W = Kp / 512: 1..8,
+// 12, 16, 24, 32 warps) and active-set capacities up to L.
 #include "common.cuh"
 #include "kernels.h"
 #include "refactor.cuh"
@@ -458,6 +459,10 @@ int lars_cta_grid(int Kp, int Lc, bool gstate) {
     case 6: return grid_w<T, 6>(smem);
     case 7: return grid_w<T, 7>(smem);
     case 8: return grid_w<T, 8>(smem);
+    case 12: return grid_w<T, 12>(smem);
+    case 16: return grid_w<T, 16>(smem);
+    case 24: return grid_w<T, 24>(smem);
+    case 32: return grid_w<T, 32>(smem);
     default: return 0;
   }
 }
@@ -475,6 +480,10 @@ cudaError_t launch_lars_cta(const LarsArgs<T>& a, int grid, cudaStream_t st) {
     case 6: return launch_w<T, 6>(a, grid, smem, st);
     case 7: return launch_w<T, 7>(a, grid, smem, st);
     case 8: return launch_w<T, 8>(a, grid, smem, st);
+    case 12: return launch_w<T, 12>(a, grid, smem, st);
+    case 16: return launch_w<T, 16>(a, grid, smem, st);
+    case 24: return launch_w<T, 24>(a, grid, smem, st);
+    case 32: return launch_w<T, 32>(a, grid, smem, st);
     default: return cudaErrorInvalidValue;
   }
 }

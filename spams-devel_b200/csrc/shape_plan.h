@@ -6,7 +6,7 @@
 //
 // A signal is coded either by one warp (Kp <= kWarpMaxKp; its correlations in
 // that warp's registers) or by one CTA of Kp / 512 warps (Kp a multiple of
-// 512).  Both run the same arithmetic in the same order, so they give the same
+// 512: any of 1..8 warps, then 12, 16, 24 or 32, up to kCtaMaxKp atoms).  Both run the same arithmetic in the same order, so they give the same
 // bits; they differ in speed: the warp kernel packs more signals per SM, the
 // CTA kernel holds larger active sets in shared memory and codes each signal
 // with more threads (lower latency when the batch is small or the active sets
@@ -22,7 +22,19 @@
 namespace sc {
 
 constexpr int kWarpMaxKp = 1024;
-constexpr int kCtaMaxKp = 4096;
+constexpr int kCtaMaxKp = 16384;
+
+// Warps per signal the CTA kernels are built for.
+inline bool cta_warps_ok(int w) { return (w >= 1 && w <= 8) || w == 12 || w == 16 || w == 24 || w == 32; }
+// The CTA kernels' layout for K atoms: K rounded up to a multiple of 512
+// whose warp count is built (beyond 4096 atoms: 6144, 8192, 12288, 16384);
+// kCtaMaxKp + 512 past the largest.
+inline int cta_pad_atoms(int K) {
+  int w = (K + 511) / 512;
+  if (w < 1) w = 1;
+  while (w <= kCtaMaxKp / 512 && !cta_warps_ok(w)) ++w;
+  return w <= kCtaMaxKp / 512 ? w * 512 : kCtaMaxKp + 512;
+}
 
 struct Shape {
   bool cta = false;  // one CTA per signal
@@ -60,7 +72,9 @@ inline Shape warp_shape(const DeviceLimits& d, int L, int cap, StateBytes state,
 }
 
 // CTA kernel: the small state is per CTA, so it can hold more atoms (up to
-// 80); the capacity shrinks in steps of 16 until two CTAs fit per SM.
+// 80); the capacity shrinks in steps of 16 until two CTAs fit per SM, where
+// two fit at all (beyond 8192 atoms the correlations alone fill most of an
+// SM's shared memory: one CTA per SM keeps the full capacity).
 // bytes(lc): one CTA's shared memory for capacity lc.
 template <typename CtaBytes>
 inline Shape cta_shape(const DeviceLimits& d, int Kp, int L, CtaBytes bytes) {
@@ -69,9 +83,9 @@ inline Shape cta_shape(const DeviceLimits& d, int Kp, int L, CtaBytes bytes) {
   s.wpb = Kp / 512;
   s.grid = 0;
   s.Lcap = std::max(1, std::min(L, 80));
-  while (s.Lcap > 16 &&
-         (bytes(s.Lcap) > d.smem_per_block || 2 * (bytes(s.Lcap) + 1024) > d.smem_per_sm))
-    s.Lcap -= 16;
+  while (s.Lcap > 16 && bytes(s.Lcap) > d.smem_per_block) s.Lcap -= 16;
+  if (2 * (bytes(std::min(s.Lcap, 16)) + 1024) <= d.smem_per_sm)
+    while (s.Lcap > 16 && 2 * (bytes(s.Lcap) + 1024) > d.smem_per_sm) s.Lcap -= 16;
   return s;
 }
 
@@ -83,7 +97,7 @@ template <typename WarpState, typename CtaBytes>
 inline std::vector<Shape> shape_candidates(const DeviceLimits& d, int Kp, int L, int kernel,
                                            WarpState state, int regw, CtaBytes bytes) {
   std::vector<Shape> v;
-  const bool warp_ok = Kp <= kWarpMaxKp, cta_ok = Kp % 512 == 0 && Kp / 512 <= 8;
+  const bool warp_ok = Kp <= kWarpMaxKp, cta_ok = Kp % 512 == 0 && cta_warps_ok(Kp / 512);
   if (warp_ok && kernel != SC_KERNEL_CTA) {
     v.push_back(warp_shape(d, L, 32, state, regw));
     if (L > 32) v.push_back(warp_shape(d, L, 64, state, regw));

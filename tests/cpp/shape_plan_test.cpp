@@ -111,6 +111,27 @@ int main() {
   CHECK(pick_fastest({1.0f, 0.90f, 0.85f}) == 2);
   CHECK(pick_fastest({1.0f, 2.0f, 0.5f}) == 2);
 
+  // the CTA kernels' layouts: multiples of 512 up to 4096 atoms, then the
+  // built warp counts 12, 16, 24, 32 (6144 .. 16384 atoms)
+  CHECK(cta_pad_atoms(1025) == 1536 && cta_pad_atoms(4096) == 4096);
+  CHECK(cta_pad_atoms(4097) == 6144 && cta_pad_atoms(6144) == 6144);
+  CHECK(cta_pad_atoms(6145) == 8192 && cta_pad_atoms(8193) == 12288);
+  CHECK(cta_pad_atoms(16384) == 16384 && cta_pad_atoms(16385) > kCtaMaxKp);
+  for (int w = 1; w <= 40; ++w)
+    CHECK(cta_warps_ok(w) == ((w <= 8) || w == 12 || w == 16 || w == 24 || w == 32));
+  {
+    // 16384 atoms: 64 KB of correlations per CTA; two CTAs never fit, so the
+    // capacity is not cut for them
+    DeviceLimits d{148, 227 * 1024, 228 * 1024};
+    auto bytes = [](int lc) { return (size_t)16384 * 4 * 2 + (size_t)lc * (lc + 1) * 4 + 4096; };
+    const Shape s = cta_shape(d, 16384, 200, bytes);
+    CHECK(s.cta && s.wpb == 32 && s.Lcap == 80);
+    // 2048 atoms: two CTAs fit once the capacity is cut to 64 or below
+    auto small = [](int lc) { return (size_t)2048 * 4 * 2 + (size_t)lc * (lc + 1) * 4 * 30; };
+    const Shape t = cta_shape(d, 2048, 200, small);
+    CHECK(t.Lcap <= 64 && 2 * (small(t.Lcap) + 1024) <= d.smem_per_sm);
+  }
+
   // host-array chunking: contiguous chunks covering [0, n), the first one half
   // the others with the copy pipeline
   auto covers = [](const ChunkPlan& c) {

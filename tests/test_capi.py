@@ -82,15 +82,15 @@ def test_c_abi_rejects_bad_counts_before_touching_the_device():
     assert "either provide L, eps or lambda" in _lib.last_error()
 
 
-def test_dictionaries_beyond_4096_atoms_are_rejected_before_the_device():
-    """Up to 1024 atoms one warp codes a signal, up to 4096 one CTA; larger
+def test_dictionaries_beyond_16384_atoms_are_rejected_before_the_device():
+    """Up to 1024 atoms one warp codes a signal, up to 16384 one CTA; larger
     dictionaries are refused with SC_ERR_UNSUPPORTED (not coded on the CPU)."""
     X = np.asfortranarray(np.random.randn(8, 3).astype(np.float32))
-    D = np.asfortranarray(np.random.randn(8, 4097).astype(np.float32))
+    D = np.asfortranarray(np.random.randn(8, 16385).astype(np.float32))
     with pytest.raises(spams_b200.ScError) as e:
         spams_b200.omp(X, D, L=2)
     assert e.value.status == _lib.SC_ERR_UNSUPPORTED
-    assert "4096" in str(e.value)
+    assert "16384" in str(e.value)
     with pytest.raises(spams_b200.ScError) as e:
         spams_b200.lasso(X, D, lambda1=0.1)
     assert e.value.status == _lib.SC_ERR_UNSUPPORTED

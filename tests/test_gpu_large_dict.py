@@ -1,8 +1,8 @@
-"""Dictionaries of 1025 to 4096 atoms: the CTA-per-signal kernels.
+"""Dictionaries of 1025 to 16384 atoms: the CTA-per-signal kernels.
 
 Beyond 1024 atoms the correlations of one signal no longer fit one warp's
 registers, so one CTA of Kp / 512 warps codes a signal (Kp = K rounded up to
-512).  The same seeded-oracle parity as the warp kernels: exact support and
+512 up to 4096 atoms, then to 6144, 8192, 12288 or 16384).  The same seeded-oracle parity as the warp kernels: exact support and
 1e-9 relative error in FP64, every constraint mode, pos, the path of signal
 0, per-signal L / eps, the rerun of active sets beyond the shared-memory
 capacity, and the (Q, q) form."""
@@ -35,6 +35,31 @@ def test_lasso_and_omp_exact_support_f64(K):
     ref = O.orc_omp(X, D, L=8)
     a = spams_b200.omp(X, D, L=8)
     assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("K", [4097, 7000, 10000, 16384])
+def test_beyond_4096_atoms_exact_support_f64(K):
+    """12, 16, 24 and 32 warps per signal (Kp 6144 .. 16384), double and
+    single precision."""
+    X, D = _draw(48, K, 24, K)
+    ref = O.orc_lasso(X, D, lambda1=0.1)
+    a = spams_b200.lasso(X, D, lambda1=0.1)
+    assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+    ref = O.orc_omp(X, D, L=8)
+    if K <= 12288:
+        a = spams_b200.omp(X, D, L=8)
+        assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+    else:  # two K-vectors of doubles per signal no longer fit a block's shared memory
+        with pytest.raises(spams_b200.ScError, match="at most 12288"):
+            spams_b200.omp(X, D, L=8)
+    a32 = spams_b200.omp(X.astype(np.float32), D.astype(np.float32), L=8)
+    assert support_match(a32, ref) >= 0.95
+
+
+def test_more_than_16384_atoms_refused():
+    X, D = _draw(16, 16385, 2, 3)
+    with pytest.raises(spams_b200.ScError, match="16384"):
+        spams_b200.omp(X.astype(np.float32), D.astype(np.float32), L=4)
 
 
 @pytest.mark.parametrize("mode,lam", [(0, 1.5), (1, 20.0), (2, 0.05)])
