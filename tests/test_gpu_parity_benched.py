@@ -167,3 +167,41 @@ def test_joining_screen_exact_tie_takes_first_index(kernel):
     assert list(a.indices) == orc_first
     if ref is not None:
         np.testing.assert_allclose(a.toarray(), ref.toarray(), rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("prec", [FP32, BF16], ids=["fp32", "bf16x3"])
+def test_dictlearn_step_accumulations_vs_reference_loop(prec):
+    """A <- beta A + gamma sum a a^T and B <- beta B + gamma sum x a^T of one
+    minibatch at the benchmarked shape, against the reference's own loop body
+    (Trainer::train, dictLearn/dicts.h:526-603: Gram + ridge, multTrans,
+    coreLARS2, sort, rank-1 updates; float build) on the same minibatch."""
+    if not O.have_ref():
+        pytest.skip("the reference build is absent")
+    m, K, batch = 144, 1024, 1024
+    rng = np.random.Generator(np.random.PCG64(1))
+    pool = 8192
+    Xnp = np.asfortranarray(W.smooth_patches(pool, rng, side=12).astype(np.float32))
+    D0 = Xnp[:, rng.choice(pool, K, replace=False)]
+    D0 = np.asfortranarray(D0 / np.linalg.norm(D0, axis=0, keepdims=True), dtype=np.float32)
+    perm = rng.permutation(pool).astype(np.int32)
+    A0 = np.asfortranarray(0.01 * rng.standard_normal((K, K)).astype(np.float32))
+    B0 = np.asfortranarray(0.01 * rng.standard_normal((m, K)).astype(np.float32))
+    beta, gamma, it0 = 0.9, 1.5, 3
+
+    def cm(a):
+        return torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.float32).T)).cuda().t()
+
+    step = spams_b200.MinibatchStep(m, K, batch, lambda1=0.1, precision=prec)
+    it = torch.full((1,), it0, dtype=torch.int64, device="cuda")
+    A, B = cm(A0), cm(B0)
+    step(cm(D0), cm(Xnp), it, perm=torch.from_numpy(perm).cuda(), A=A, B=B, beta=beta,
+         gamma=gamma)
+    torch.cuda.synchronize()
+    Ar, Br = A0.copy(order="F"), B0.copy(order="F")
+    O.ref_dl_minibatch(D0, Xnp, perm, it0, batch, 0.1, Ar, Br, beta=beta, gamma=gamma)
+    ea = np.linalg.norm(A.cpu().numpy() - Ar) / np.linalg.norm(Ar)
+    eb = np.linalg.norm(B.cpu().numpy() - Br) / np.linalg.norm(Br)
+    print(f"\ndictlearn accumulations prec={prec}: A rel err {ea:.2e}, B rel err {eb:.2e}")
+    assert int(it.item()) == it0 + 1
+    assert ea <= (1e-5 if prec == FP32 else 1e-4)
+    assert eb <= (1e-5 if prec == FP32 else 1e-4)
