@@ -174,9 +174,16 @@ def test_dictlearn_step_accumulations_vs_reference_loop(prec):
     """A <- beta A + gamma sum a a^T and B <- beta B + gamma sum x a^T of one
     minibatch at the benchmarked shape, against the reference's own loop body
     (Trainer::train, dictLearn/dicts.h:526-603: Gram + ridge, multTrans,
-    coreLARS2, sort, rank-1 updates; float build) on the same minibatch."""
+    coreLARS2, sort, rank-1 updates; float build) on the same minibatch.
+
+    The accumulation is exact arithmetic on the step's own codes (checked in
+    double); the codes match the reference's float codes column by column,
+    where one column whose last atom is picked differently moves A by ~5e-3
+    (an atom of a smooth-patch dictionary), so A and B against the
+    reference's own loop are held to that scale."""
     if not O.have_ref():
         pytest.skip("the reference build is absent")
+    import scipy.sparse as ssp
     m, K, batch = 144, 1024, 1024
     rng = np.random.Generator(np.random.PCG64(1))
     pool = 8192
@@ -197,11 +204,27 @@ def test_dictlearn_step_accumulations_vs_reference_loop(prec):
     step(cm(D0), cm(Xnp), it, perm=torch.from_numpy(perm).cuda(), A=A, B=B, beta=beta,
          gamma=gamma)
     torch.cuda.synchronize()
+    assert int(it.item()) == it0 + 1
+    Ag, Bg = A.cpu().numpy().astype(np.float64), B.cpu().numpy().astype(np.float64)
+    cp, r, v = (t.cpu().numpy() for t in step.codes())
+    codes = ssp.csc_matrix((v, r, cp), shape=(K, batch)).astype(np.float64)
+    Xb = Xnp[:, perm[(np.arange(batch) + it0 * batch) % pool]].astype(np.float64)
+    # the accumulation itself, on the step's own codes
+    Ae = beta * A0.astype(np.float64) + gamma * (codes @ codes.T).toarray()
+    Be = beta * B0.astype(np.float64) + gamma * (codes @ Xb.T).T
+    assert np.linalg.norm(Ag - Ae) / np.linalg.norm(Ae) <= 1e-6
+    assert np.linalg.norm(Bg - Be) / np.linalg.norm(Be) <= 1e-6
+    # the codes against the reference's float coreLARS2 on the same minibatch
+    refc = O.ref_lasso(np.asfortranarray(Xb, np.float32), D0, lambda1=0.1, L=min(m, K),
+                       numThreads=-1)
+    sm, fro, _, _ = err_report(codes, refc)
+    # A and B against the reference's own loop
     Ar, Br = A0.copy(order="F"), B0.copy(order="F")
     O.ref_dl_minibatch(D0, Xnp, perm, it0, batch, 0.1, Ar, Br, beta=beta, gamma=gamma)
-    ea = np.linalg.norm(A.cpu().numpy() - Ar) / np.linalg.norm(Ar)
-    eb = np.linalg.norm(B.cpu().numpy() - Br) / np.linalg.norm(Br)
-    print(f"\ndictlearn accumulations prec={prec}: A rel err {ea:.2e}, B rel err {eb:.2e}")
-    assert int(it.item()) == it0 + 1
-    assert ea <= (1e-5 if prec == FP32 else 1e-4)
-    assert eb <= (1e-5 if prec == FP32 else 1e-4)
+    ea = np.linalg.norm(Ag - Ar) / np.linalg.norm(Ar)
+    eb = np.linalg.norm(Bg - Br) / np.linalg.norm(Br)
+    print(f"\ndictlearn step prec={prec}: codes vs reference float support {sm:.4f}, "
+          f"rel err {fro:.2e}; A rel err {ea:.2e}, B rel err {eb:.2e}")
+    assert sm >= 0.995
+    assert fro <= (1e-4 if prec == FP32 else 1e-3)
+    assert ea <= 2e-2 and eb <= 2e-2
