@@ -267,10 +267,10 @@ static std::vector<Shape> candidates_for(const DeviceCtx& c, bool lars, int Kp, 
 }
 
 struct TuneKey {
-  int lars, dbl, Kp, lclass, nclass, kernel;
+  int lars, dbl, Kp, lclass, nclass, kernel, masked;
   bool operator<(const TuneKey& o) const {
-    return std::tie(lars, dbl, Kp, lclass, nclass, kernel) <
-           std::tie(o.lars, o.dbl, o.Kp, o.lclass, o.nclass, o.kernel);
+    return std::tie(lars, dbl, Kp, lclass, nclass, kernel, masked) <
+           std::tie(o.lars, o.dbl, o.Kp, o.lclass, o.nclass, o.kernel, o.masked);
   }
 };
 static std::mutex g_tune_mu;
@@ -474,7 +474,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // unit per warp (warp kernels) or CTA (CTA kernels, whose grid is then fixed
   // here)
   const bool refac = sizeof(T) == 4 && p.refactor != 0 && !p.chol;
-  if (refac)
+  if (refac || p.hmask)  // per-CTA scratch (refactor, masked products): a fixed grid
     for (Shape& sh : cands)
       if (sh.cta)
         sh.grid = p.lars ? lars_cta_grid<T>(Kp, sh.Lcap, false) : omp_cta_grid<T>(Kp, sh.Lcap, false);
@@ -563,7 +563,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     rf_units = (int)units;
   }
   // masked variants: Dᵀ, the chunk's mask / classes / scaled parameters, and
-  // one m-vector of scratch per warp of the largest launch
+  // one m-vector of scratch per warp (warp kernels) or CTA (CTA kernels) of
+  // the largest launch
   MaskArgs<T> mk{};
   if (p.hmask) {
     mk.m = p.m;
@@ -578,7 +579,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     SC_TRY(c.mvec.reserve((size_t)nc * sizeof(T)));
     size_t warps = 0;
     for (const Shape& sh : cands) {
-      warps = std::max(warps, (size_t)sh.grid * sh.wpb);
+      warps = std::max(warps, (size_t)sh.grid * (sh.cta ? 1 : sh.wpb));
       const Ovf ov = ovf_plan(sh);
       warps = std::max(warps, (size_t)ov.grid * ov.wpb);
     }
@@ -671,7 +672,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   // kernel family: a single candidate, the cached choice of an earlier call,
   // the static rule, or timed on the first chunk (tune)
   int chosen = cands.size() == 1 ? 0 : -1;
-  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, tune_lclass(p.L), 0, p.kernel};
+  TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, tune_lclass(p.L), 0, p.kernel,
+              p.hmask ? 1 : 0};
   {
     int64_t c0 = std::min<int64_t>(nc, p.n), cls = 0;
     while (c0 > 1) { c0 >>= 1; ++cls; }
@@ -998,15 +1000,6 @@ int pad_atoms(int K) {
 static int pad_atoms_for(int K, const sc_options* opt) {
   return opt && opt->kernel == SC_KERNEL_CTA ? cta_pad_atoms(K) : pad_atoms(K);
 }
-// The masked variants run on the warp-per-signal kernels only.
-static sc_status check_mask(int K, const uint8_t* mask, const sc_options* opt) {
-  if (!mask) return SC_OK;
-  if (pad128(K) > kWarpMaxKp)
-    return fail(SC_ERR_UNSUPPORTED, "masked coding takes at most %d atoms (K=%d)", kWarpMaxKp, K);
-  if (opt && opt->kernel == SC_KERNEL_CTA)
-    return fail(SC_ERR_UNSUPPORTED, "masked coding runs on the warp-per-signal kernels only");
-  return SC_OK;
-}
 static sc_status check_kernel(int K, const sc_options* opt) {
   if (opt && opt->kernel == SC_KERNEL_WARP && pad128(K) > kWarpMaxKp)
     return fail(SC_ERR_UNSUPPORTED, "the warp-per-signal kernels take at most %d atoms (K=%d)",
@@ -1155,7 +1148,6 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   L = std::min(m, std::min(L, K));
   if (n == 0 || L <= 0) return emit_empty<T>(K, n, out);
   SC_TRY(check_omp_atoms<T>(K));
-  SC_TRY(check_mask(K, mask, opt));
 
   SC_TRY(check_opts<T>(opt));
   SC_TRY(check_kernel(K, opt));
@@ -1267,7 +1259,6 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);
   SC_TRY(check_atoms(K));
-  SC_TRY(check_mask(K, mask, opt));
 
   SC_TRY(check_opts<T>(opt));
   SC_TRY(check_kernel(K, opt));

@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "refactor.cuh"
+#include "masked.cuh"
 #include "lars_screen.cuh"
 
 namespace sc {
@@ -50,7 +51,7 @@ __host__ __device__ inline size_t lars_cta_smem(int Kp, int Lc, size_t esz, int 
          (gstate ? 0 : lars_cta_state(Lc, esz));
 }
 
-template <typename T, int W>
+template <typename T, int W, bool MASKED>
 __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   constexpr int NV = 4;  // 128-row chunks per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -105,6 +106,11 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
     const int64_t sig = a.sig_list ? a.sig_list[job] : (int64_t)job;
     const T constraint = a.vConstraint ? a.vConstraint[sig] : a.constraint;
     T* path = (a.path && sig == 0) ? a.path : nullptr;
+    // masked variant: no row observed -> empty code; some -> the masked Gram
+    const int mflag = MASKED ? (int)a.mk.flag[sig] : 2;
+    const bool partial = MASKED && mflag == 1;
+    const uint8_t* mrow = MASKED ? a.mk.mask + (size_t)sig * a.mk.m : nullptr;
+    T* mw = MASKED ? a.mk.work + (size_t)blockIdx.x * a.mk.mpad : nullptr;
 
     // ---- load D^T x (own rows) and find the first atom
     const T* dtx = a.DtX + (size_t)sig * Kp;
@@ -147,7 +153,7 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
 
     int cnt = 0;
     bool overflow = false;
-    bool skip = L <= 0;
+    bool skip = L <= 0 || mflag == 0;
     if (!skip) {
       const T dc = sDtR[cur];
       if (mode == 2 && fabs(dc) < constraint) skip = true;
@@ -170,8 +176,15 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
           if (gw == 0) {
             if (lane == 0) sInd[i] = cur;
             __syncwarp();
-            const T* gcol = a.G + (size_t)cur * Kp;
-            for (int j = lane; j <= i; j += 32) sG[j] = gcol[sInd[j]];
+            if (partial) {
+              for (int j = 0; j <= i; ++j) {
+                const T g = masked_gram(a.mk, mrow, sInd[j], cur);
+                if (lane == 0) sG[j] = g;
+              }
+            } else {
+              const T* gcol = a.G + (size_t)cur * Kp;
+              for (int j = lane; j <= i; j += 32) sG[j] = gcol[sInd[j]];
+            }
             __syncwarp();
             if (i == 0) {
               if (lane == 0) sInv[0] = T(1) / sG[0];
@@ -185,7 +198,7 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
               // a small pivot loses digits in the update: rebuild the inverse in FP64
               bool refactored = false;
               if (sizeof(T) == 4 && a.refactor && i < a.rf_cap && (int)blockIdx.x < a.rf_units &&
-                  (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
+                  !partial && (a.refactor == 2 || !(piv > T(kRefactorPivot) * sG[i]))) {
                 double* rs = a.rf_scratch + (size_t)blockIdx.x * a.rf_cap * a.rf_cap;
                 refactored = refactor_inverse<T>(a.G, Kp, sInd, i + 1, sInv, ldi, rs);
               }
@@ -238,12 +251,16 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
         for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int e = 0; e < 4; ++e) A[v][e] = 0;
+        if (partial) {
+          masked_gram_times_cta<T, NV, W>(a.mk, mrow, mw, Kp, rbase, sInd, sU, 1, i + 1, A);
+        } else {
 #pragma unroll 4
-        for (int j = 0; j <= i; ++j) {
-          const T uj = sU[j];
-          const T* gc = a.G + (size_t)sInd[j] * Kp + rbase + lane * 4;
+          for (int j = 0; j <= i; ++j) {
+            const T uj = sU[j];
+            const T* gc = a.G + (size_t)sInd[j] * Kp + rbase + lane * 4;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
+            for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), uj);
+          }
         }
         // ---- joining candidates of the own rows (lars_screen.cuh)
         {
@@ -394,16 +411,16 @@ __device__ __forceinline__ void lars_cta_body(const LarsArgs<T> a) {
   }
 }
 
-template <typename T, int W>
+template <typename T, int W, bool MASKED = false>
 __global__ void __launch_bounds__(W * 32) lars_cta_kernel(const LarsArgs<T> a) {
-  lars_cta_body<T, W>(a);
+  lars_cta_body<T, W, MASKED>(a);
 }
 // The same kernel built with at most 64 registers, taken only where it keeps
 // more CTAs resident (2.57 -> 2.34 ms per 20k signals on 4096 atoms); where
 // shared memory limits residency its spills only cost time.
-template <typename T, int W>
+template <typename T, int W, bool MASKED = false>
 __global__ void __launch_bounds__(W * 32, 32 / W) lars_cta_kernel_lb(const LarsArgs<T> a) {
-  lars_cta_body<T, W>(a);
+  lars_cta_body<T, W, MASKED>(a);
 }
 
 // The build a launch uses: register-bounded where that keeps more CTAs
@@ -411,16 +428,17 @@ __global__ void __launch_bounds__(W * 32, 32 / W) lars_cta_kernel_lb(const LarsA
 // matches the residency of the kernel it runs).  Unlike the warp kernel, this
 // one has no constraint-mode specialisation: a PENALTY-only build ran slower
 // (1.22 -> 1.47 ms per 1024-signal minibatch on 1024 atoms).
-template <typename T, int W>
+template <typename T, int W, bool MASKED = false>
 static auto pick_kernel(size_t smem) {
-  auto k = lars_cta_kernel<T, W>;
-  if constexpr (sizeof(T) == 4) k = more_resident(k, lars_cta_kernel_lb<T, W>, W * 32, smem);
+  auto k = lars_cta_kernel<T, W, MASKED>;
+  if constexpr (sizeof(T) == 4)
+    k = more_resident(k, lars_cta_kernel_lb<T, W, MASKED>, W * 32, smem);
   return k;
 }
 
 template <typename T, int W>
 static cudaError_t launch_w(const LarsArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-  auto k = pick_kernel<T, W>(smem);
+  auto k = a.mk.mask ? pick_kernel<T, W, true>(smem) : pick_kernel<T, W, false>(smem);
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);

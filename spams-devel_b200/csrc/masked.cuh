@@ -62,4 +62,41 @@ __device__ __forceinline__ void masked_gram_times(const MaskArgs<T>& mk, const u
   __syncwarp();  // w is rewritten at the next step
 }
 
+// CTA-collective form for the CTA-per-signal kernels (every thread of the CTA
+// calls it): A += G_m(:, ind[0:len]) u over this warp's rows
+// (r = rbase + 128 v + 4 lane + e); w: the CTA's mpad-vector of scratch.  The
+// same sums in the same order as masked_gram_times, so both kernel families
+// give the same bits.
+template <typename T, int NV, int W>
+__device__ __forceinline__ void masked_gram_times_cta(const MaskArgs<T>& mk, const uint8_t* mrow,
+                                                      T* w, int Kp, int rbase, const int* ind,
+                                                      const T* u, int ustride, int len,
+                                                      T (&A)[NV][4]) {
+  const int lane = threadIdx.x & 31;
+  for (int r = threadIdx.x; r < mk.m; r += W * 32) {
+    T s = 0;
+    if (mrow[r])
+      for (int j = 0; j < len; ++j) s += mk.D[(size_t)ind[j] * mk.m + r] * u[(size_t)j * ustride];
+    w[r] = s;
+  }
+  __syncthreads();
+  for (int r = 0; r < mk.m; ++r) {
+    const T wr = w[r];
+    if (wr == T(0)) continue;
+    const T* dt = mk.Dt + (size_t)r * Kp + rbase + lane * 4;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(dt + v * 128), wr);
+  }
+  for (int j = 0; j < len; ++j) {
+    const int c = ind[j];
+    const T add = mk.ridge * u[(size_t)j * ustride];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (rbase + v * 128 + lane * 4 + e == c) A[v][e] += add;
+  }
+  __syncthreads();  // w is rewritten at the next step
+}
+
 }  // namespace sc

@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "refactor.cuh"
+#include "masked.cuh"
 
 namespace sc {
 
@@ -25,7 +26,7 @@ __host__ __device__ inline size_t omp_cta_smem(int Kp, int Lc, size_t esz, int W
          (gstate ? 0 : omp_cta_state(Lc, esz));
 }
 
-template <typename T, int W>
+template <typename T, int W, bool MASKED>
 __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
   constexpr int NV = 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -68,6 +69,11 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
     const T lambda = a.vLambda ? a.vLambda[sig] : a.lambda;
     T normX = a.norms[sig];
     T* path = (a.path && sig == 0) ? a.path : nullptr;
+    // masked variant: no row observed -> empty code; some -> the masked Gram
+    const int mflag = MASKED ? (int)a.mk.flag[sig] : 2;
+    const bool partial = MASKED && mflag == 1;
+    const uint8_t* mrow = MASKED ? a.mk.mask + (size_t)sig * a.mk.m : nullptr;
+    T* mw = MASKED ? a.mk.work + (size_t)blockIdx.x * a.mk.mpad : nullptr;
 
     // ---- load D^T x; norm = 1; first choice = first max |D^T x|
     const T* dtx = a.DtX + (size_t)sig * Kp;
@@ -106,7 +112,7 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
     int j = 0;
     bool overflow = false;
     uint32_t act = 0;
-    const bool started = !(normX <= eps || L <= 0);
+    const bool started = !(normX <= eps || L <= 0 || mflag == 0);
     if (started) {
       for (j = 0; j < L; ++j) {
         if (j >= Lc) { overflow = true; break; }
@@ -119,7 +125,7 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
         // (the decision is the same in every warp: nc comes from shared memory)
         bool refactored = false;
         if (sizeof(T) == 4 && a.refactor && j < a.rf_cap && (int)blockIdx.x < a.rf_units &&
-            (a.refactor == 2 || !(nc > T(kRefactorPivot)))) {
+            !partial && (a.refactor == 2 || !(nc > T(kRefactorPivot)))) {
           if (gw == 0) {
             if (lane == 0) sInd[j] = c;
             __syncwarp();
@@ -146,8 +152,15 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
           __syncwarp();
         } else if (gw == 0) {
           if (lane == 0) { sRUn[j] = RU; sInd[j] = c; }
-          const T* gcol = a.G + (size_t)c * Kp;
-          for (int l = lane; l < j; l += 32) sGg[l] = gcol[sInd[l]];
+          if (partial) {
+            for (int l = 0; l < j; ++l) {
+              const T g = masked_gram(a.mk, mrow, sInd[l], c);
+              if (lane == 0) sGg[l] = g;
+            }
+          } else {
+            const T* gcol = a.G + (size_t)c * Kp;
+            for (int l = lane; l < j; l += 32) sGg[l] = gcol[sInd[l]];
+          }
           __syncwarp();
           for (int k = lane; k < j; k += 32) {
             T s = 0;
@@ -179,12 +192,16 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
         for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int e = 0; e < 4; ++e) A[v][e] = 0;
+        if (partial) {
+          masked_gram_times_cta<T, NV, W>(a.mk, mrow, mw, Kp, rbase, sInd, sUn + j, ldu, j + 1, A);
+        } else {
 #pragma unroll 4
-        for (int l = 0; l <= j; ++l) {
-          const T ul = sUn[(size_t)l * ldu + j];
-          const T* gc = a.G + (size_t)sInd[l] * Kp + rbase + lane * 4;
+          for (int l = 0; l <= j; ++l) {
+            const T ul = sUn[(size_t)l * ldu + j];
+            const T* gc = a.G + (size_t)sInd[l] * Kp + rbase + lane * 4;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), ul);
+            for (int v = 0; v < NV; ++v) axpy4(A[v], ldg4(gc + v * 128), ul);
+          }
         }
         const T mRU = -sRUn[j];
         T ck[4];
@@ -261,9 +278,9 @@ __device__ __forceinline__ void omp_cta_body(const OmpArgs<T> a) {
   }
 }
 
-template <typename T, int W>
+template <typename T, int W, bool MASKED = false>
 __global__ void __launch_bounds__(W * 32) omp_cta_kernel(const OmpArgs<T> a) {
-  omp_cta_body<T, W>(a);
+  omp_cta_body<T, W, MASKED>(a);
 }
 // The same kernel built with at most 64 registers, so that up to 32 warps per
 // SM can be resident (the per-step Gram-column reads from L2 need the
@@ -271,15 +288,22 @@ __global__ void __launch_bounds__(W * 32) omp_cta_kernel(const OmpArgs<T> a) {
 // where shared memory is not the limit (small active-set capacity): 1.86 ->
 // 1.40 ms per 20k signals of 18-step OMP on 1024 atoms, 5.87 -> 5.15 on 4096;
 // with an 80-atom state it fits no more CTAs and its spills cost 5%.
-template <typename T, int W>
+template <typename T, int W, bool MASKED = false>
 __global__ void __launch_bounds__(W * 32, 32 / W) omp_cta_kernel_lb(const OmpArgs<T> a) {
-  omp_cta_body<T, W>(a);
+  omp_cta_body<T, W, MASKED>(a);
+}
+
+template <typename T, int W, bool MASKED>
+static auto pick_omp_cta(size_t smem) {
+  auto k = omp_cta_kernel<T, W, MASKED>;
+  if constexpr (sizeof(T) == 4)
+    k = more_resident(k, omp_cta_kernel_lb<T, W, MASKED>, W * 32, smem);
+  return k;
 }
 
 template <typename T, int W>
 static cudaError_t launch_w(const OmpArgs<T>& a, int grid, size_t smem, cudaStream_t st) {
-  auto k = omp_cta_kernel<T, W>;
-  if constexpr (sizeof(T) == 4) k = more_resident(k, omp_cta_kernel_lb<T, W>, W * 32, smem);
+  auto k = a.mk.mask ? pick_omp_cta<T, W, true>(smem) : pick_omp_cta<T, W, false>(smem);
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess) return e;
   e = fill_grid(k, W * 32, smem, &grid);

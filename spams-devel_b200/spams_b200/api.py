@@ -219,7 +219,7 @@ def _mask_of(B, m: int, n: int, name: str) -> np.ndarray:
 
 
 def ompMask(X, D, B, L=None, eps=None, lambda1=None, return_reg_path=False, numThreads=-1,
-            precision=None, device=0):
+            precision=None, device=0, kernel=None):
     """OMP of every column of X on its observed rows (swig/python/spams.py:201-232).
 
     B (m x n, boolean) marks the observed rows of each signal; a signal is
@@ -243,7 +243,7 @@ def ompMask(X, D, B, L=None, eps=None, lambda1=None, return_reg_path=False, numT
     out = CscF64() if f64 else CscF32()
     ct = C.c_double if f64 else C.c_float
     fn = _lib.lib().sc_omp_mask_f64 if f64 else _lib.lib().sc_omp_mask_f32
-    o = _opts(precision, device)
+    o = _opts(precision, device, kernel=kernel)
     st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Bm, C.c_uint8), _ptr(Lv, C.c_int32), nL,
             _ptr(ev, ct), nE, _ptr(lv, ct), nLa, numThreads, _ptr(path, ct), C.byref(o),
             C.byref(out))
@@ -253,7 +253,7 @@ def ompMask(X, D, B, L=None, eps=None, lambda1=None, return_reg_path=False, numT
 
 
 def lassoMask(X, D, B, L=-1, lambda1=None, lambda2=0., mode=SC_PENALTY, pos=False,
-              numThreads=-1, verbose=False, precision=None, device=0):
+              numThreads=-1, verbose=False, precision=None, device=0, kernel=None):
     """LARS-Lasso of every column of X on its observed rows
     (swig/python/spams.py:144-153): B (m x n, boolean) marks the observed rows;
     PENALTY / L2ERROR constraints scale by the observed fraction."""
@@ -271,7 +271,7 @@ def lassoMask(X, D, B, L=-1, lambda1=None, lambda2=0., mode=SC_PENALTY, pos=Fals
     out = CscF64() if f64 else CscF32()
     ct = C.c_double if f64 else C.c_float
     fn = _lib.lib().sc_lasso_mask_f64 if f64 else _lib.lib().sc_lasso_mask_f32
-    o = _opts(precision, device)
+    o = _opts(precision, device, kernel=kernel)
     st = fn(_ptr(X, ct), m, n, _ptr(D, ct), K, _ptr(Bm, C.c_uint8), int(L), float(lambda1),
             float(lambda2), int(mode), int(bool(pos)), numThreads, C.byref(o), C.byref(out))
     _raise(st)

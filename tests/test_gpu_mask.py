@@ -92,10 +92,33 @@ def test_masked_path_of_the_first_signal():
     np.testing.assert_allclose(path, rpath, rtol=1e-8, atol=1e-10)
 
 
+@pytest.mark.parametrize("m,K", [(32, 1500), (40, 2048), (24, 5000)])
+def test_masked_on_the_cta_kernels_f64(m, K):
+    """Beyond 1024 atoms the masked products run on the CTA-per-signal
+    kernels (Kp / 512 warps per signal): the same exact supports and FP64
+    values against the oracle."""
+    X, D, B = _draw(m, K, 60, K + 3)
+    for kw in (dict(L=6), dict(L=12, lambda1=0.01)):
+        ref = O.orc_omp_mask(X, D, B, **kw)
+        a = spams_b200.ompMask(X, D, B, **kw)
+        assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+    for kw in (dict(lambda1=0.05), dict(lambda1=0.3, mode=1, pos=True)):
+        ref = _nz(O.orc_lasso_mask(X, D, B, **kw))
+        a = _nz(spams_b200.lassoMask(X, D, B, **kw))
+        assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_masked_warp_and_cta_kernels_give_the_same_bits(dt):
+    X, D, B = _draw(48, 512, 300, 17)
+    Xd, Dd = X.astype(dt), D.astype(dt)
+    _same(spams_b200.ompMask(Xd, Dd, B, L=10, kernel="warp"),
+          spams_b200.ompMask(Xd, Dd, B, L=10, kernel="cta"))
+    _same(spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="warp"),
+          spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="cta"))
+
+
 def test_masked_limits():
-    X, D, B = _draw(32, 1500, 10, 3)
-    with pytest.raises(spams_b200.ScError) as e:
-        spams_b200.ompMask(X, D, B, L=4)
-    assert e.value.status == _lib.SC_ERR_UNSUPPORTED
+    X, D, B = _draw(32, 150, 10, 3)
     with pytest.raises(ValueError, match="non acceptable dimensions"):
         spams_b200.lassoMask(X, D, B[:, :5], lambda1=0.1)
