@@ -245,8 +245,8 @@ sc_status sc_corr_f32_dev(const float* dD, int m, int K, const float* dX, int64_
  *   256 + 2 * r(2 * m64 * K) + 2 * r(2 * m64 * n) bytes must fit in 16 MiB,
  *   m64 = m rounded up to a multiple of 64 and r(b) = b rounded up to a
  *   multiple of 256 (larger calls return SC_ERR_CAPACITY; split X by columns).
- *   The first call on a device looks up the array's address there (make it
- *   before any stream capture).  All calls share the array: calls that
+ *   The first call on a device looks up the array's address there
+ *   (cudaGetSymbolAddress).  All calls share the array: calls that
  *   overlap on the GPU race and must be serialised.  Every call synchronises
  *   its stream (it reads back the pipeline's timeout flag) and returns after
  *   the stream has finished the product.  No cudaMalloc / cudaFree or other

@@ -13,8 +13,8 @@
 // The scratch is the file-scope array below: kNoAllocScratchBytes (16 MiB) of
 // device memory that every GPU which loads the library holds until the
 // process exits.  Its device address is looked up once per device, on the
-// first call made with that device current (cudaGetSymbolAddress); make that
-// first call before any stream capture.  All calls share the array and it
+// first call made with that device current (cudaGetSymbolAddress).  All
+// calls share the array and it
 // keeps the last call's contents, so calls that overlap on the GPU (two
 // streams, or two host threads) race: serialise them.
 #include <cuda_runtime.h>
