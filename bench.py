@@ -345,8 +345,12 @@ def run_ours(args) -> None:
     Xh = torch.empty((n, M), dtype=torch.float32, pin_memory=True)
     Xh.numpy()[:] = Xf.T
     Xnp = Xh.numpy().T  # Fortran-ordered view, pinned
-    for _ in range(max(1, args.warmup // 2)):
-        spams_b200.lasso(Xnp, Df, lambda1=LAMBDA, precision=prec, kernel=KERNEL)
+    # warm-up in the steady state of a caller that keeps each result until the
+    # next one arrives (two results alive: the result pool holds two sets of
+    # page-locked blocks from then on)
+    a = None
+    for _ in range(max(2, args.warmup // 2)):
+        a = spams_b200.lasso(Xnp, Df, lambda1=LAMBDA, precision=prec, kernel=KERNEL)
     barrier()
     e2e_t = []
     e2e_steps = max(1, min(args.steps, 10))
@@ -506,7 +510,9 @@ def uneven_omp_result(n: int, steps: int, warmup: int, precision: str, cpu_secon
     Xnp = Xh.numpy().T
     Dnp = np.asfortranarray(D.cpu().numpy())
     Lnp, Enp = Lv.cpu().numpy(), eps.cpu().numpy()
-    spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
+    a = None
+    for _ in range(2):  # two results alive, as in the timed loop
+        a = spams_b200.omp(Xnp, Dnp, L=Lnp, eps=Enp, precision=prec)
     e2e_t = []
     for _ in range(max(1, min(steps, 3))):
         t0 = time.perf_counter()
