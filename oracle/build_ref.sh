@@ -11,14 +11,13 @@
 # The ILP64 numpy OpenBLAS must not be used: the reference's INTT is int.
 #
 # Usage: oracle/build_ref.sh [REFERENCE_DIR]
-#   REFERENCE_DIR: the argument, else $SPAMS_REFERENCE_DIR, else the read-only
-#   checkout this recipe was written against (/root/reference).  Exits 2 when
-#   no reference sources are found there.
+#   REFERENCE_DIR: the argument, else $SPAMS_REFERENCE_DIR.  Exits 2 when
+#   neither is given or no reference sources are found there.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-${SPAMS_REFERENCE_DIR:-/root/reference}}"
+REF="${1:-${SPAMS_REFERENCE_DIR:-}}"
 OUT="$HERE/_ref"
-if [ ! -d "$REF/decomp" ]; then
+if [ -z "$REF" ] || [ ! -d "$REF/decomp" ]; then
   echo "build_ref: reference sources not found at $REF" >&2
   exit 2
 fi

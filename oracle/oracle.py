@@ -22,7 +22,7 @@ import scipy.sparse as ssp
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_SO = os.path.join(HERE, "liborc.so")
 REF_SO = os.path.join(HERE, "_ref", "libspams_ref.so")
-# The reference checkout: SPAMS_REFERENCE_DIR, else build_ref.sh's own default.
+# The reference checkout: SPAMS_REFERENCE_DIR (or build_ref's argument).
 REFERENCE_DIR = os.environ.get("SPAMS_REFERENCE_DIR")
 
 
@@ -37,8 +37,8 @@ def build_orc() -> str:
 def build_ref(reference_dir: str | None = REFERENCE_DIR) -> str | None:
     """Compile oracle/_ref from the reference sources when they are present.
 
-    ``reference_dir`` (or SPAMS_REFERENCE_DIR) names the checkout; without it
-    build_ref.sh looks in its own default location.  The script exits 2 when
+    ``reference_dir`` (or SPAMS_REFERENCE_DIR) names the checkout; without
+    either nothing is built.  The script exits 2 when
     it finds no sources, and an existing build is then kept as it is.
     """
     deps = [os.path.join(HERE, "ref_driver.cpp"), os.path.join(HERE, "build_ref.sh")]
