@@ -156,8 +156,8 @@ sc_status sc_omp_f64(const double* X, int m, int64_t n, const double* D, int K,
  *   ols / cholesky select the reference's Cholesky implementation (lasso<T>
  *   -> coreLARS + downDateLasso, decomp/decomp.h:735-1203; ols implies it, as
  *   in _lassoD): its own stopping rules in all three modes, and with ols the
- *   final least-squares fit on the support.  Up to 1024 atoms
- *   (SC_ERR_UNSUPPORTED beyond). */
+ *   final least-squares fit on the support.  Dictionaries as the coding
+ *   kernels (one warp per signal up to 1024 atoms, one CTA beyond). */
 sc_status sc_lasso_f32(const float* X, int m, int64_t n, const float* D, int K,
                        int L, float lambda1, float lambda2, int mode, int pos,
                        int ols, int numThreads, int max_length_path,
@@ -267,7 +267,8 @@ sc_status sc_corr_bf16x3_noalloc_f32(const float* dD, int m, int K, const float*
  *                    lasso_mask, decomp/decomp.h:1466-1561): ridge
  *                    max(lambda2, 1e-10); PENALTY and L2ERROR constraints scale
  *                    by the observed fraction; L clamped as in _lassoD; no path.
- * Dictionaries up to 1024 atoms (SC_ERR_UNSUPPORTED beyond). */
+ * Dictionaries as the coding kernels (one warp per signal up to 1024 atoms,
+ * one CTA beyond). */
 sc_status sc_omp_mask_f32(const float* X, int m, int64_t n, const float* D, int K,
                           const uint8_t* mask, const int* L, int64_t nL, const float* eps,
                           int64_t nEps, const float* lambda, int64_t nLambda, int numThreads,

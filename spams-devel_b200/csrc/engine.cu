@@ -265,6 +265,18 @@ static std::vector<Shape> candidates_for(const DeviceCtx& c, bool lars, int Kp, 
                    : (lars ? lars_max_warps_per_sm<T>(Kp) : omp_max_warps_per_sm<T>(Kp));
   return shape_candidates(d, Kp, L, kernel, state, regw, bytes);
 }
+// The Cholesky implementation's shape: the warp kernel (4 warps per block, a
+// 32-atom state) up to kWarpMaxKp atoms unless the CTA family is asked for,
+// else the CTA kernel with the capacity cta_shape gives its shared memory.
+template <typename T>
+static Shape chol_shape(const DeviceCtx& c, int Kp, int L, int kernel) {
+  if (Kp <= kWarpMaxKp && kernel != SC_KERNEL_CTA) return Shape{false, std::min(L, 32), 4, 0};
+  DeviceLimits d;
+  d.num_sms = c.num_sms;
+  d.smem_per_block = (size_t)c.smem_per_block;
+  d.smem_per_sm = (size_t)c.smem_per_sm;
+  return cta_shape(d, Kp, L, [&](int lc) { return lars_chol_cta_smem_bytes(Kp, lc, sizeof(T), false); });
+}
 
 struct TuneKey {
   int lars, dbl, Kp, lclass, nclass, kernel, masked;
@@ -465,10 +477,12 @@ template <typename T>
 static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, const T* dG,
                               HostSink<T>* sink, int* d_capflag, Prof& pr) {
   const int Kp = p.Kp;
-  // the Cholesky implementation has one kernel: warps of 4 per block, a
-  // 32-atom state in shared memory, the overflow pass with capacity L
+  // the Cholesky implementation has one shape per layout: up to 1024 atoms
+  // warps of 4 per block with a 32-atom state in shared memory, beyond (or
+  // with the CTA family asked for) one CTA per signal; the overflow pass
+  // with capacity L
   std::vector<Shape> cands =
-      p.chol ? std::vector<Shape>{Shape{false, std::min(p.L, 32), 4, 0}}
+      p.chol ? std::vector<Shape>{chol_shape<T>(c, Kp, p.L, p.kernel)}
              : candidates_for<T>(c, p.lars, Kp, p.L, p.kernel);
   // FP64 refactor of the single-precision state (refactor.cuh): one scratch
   // unit per warp (warp kernels) or CTA (CTA kernels, whose grid is then fixed
@@ -535,7 +549,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     Ovf o;
     o.wpb = sh.cta ? 1 : 4;
     const size_t per =
-        p.chol ? lars_chol_state_bytes(Kp, p.L, sizeof(T))
+        p.chol ? (sh.cta ? lars_chol_cta_gstate_bytes(p.L, sizeof(T))
+                         : lars_chol_state_bytes(Kp, p.L, sizeof(T)))
         : sh.cta ? (p.lars ? lars_cta_gstate_bytes<T>(p.L, 1) : omp_cta_gstate_bytes<T>(p.L, 1))
                  : (p.lars ? lars_state_bytes(Kp, p.L, sizeof(T)) : omp_state_bytes(Kp, p.L, sizeof(T)));
     o.grid = sh.cta ? 2 * c.num_sms : c.num_sms;
@@ -835,7 +850,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
         a.rf_cap = refactor_cap(shp.Lcap);
         a.rf_units = refac ? rf_units : 0;
         a.ols = p.ols ? 1 : 0;
-        if (p.chol) SC_CUDA(launch_lars_chol<T>(a, shp.grid, shp.wpb, st));
+        if (p.chol && shp.cta) SC_CUDA(launch_lars_chol_cta<T>(a, shp.grid, st));
+        else if (p.chol) SC_CUDA(launch_lars_chol<T>(a, shp.grid, shp.wpb, st));
         else if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, shp.grid, st));
         else SC_CUDA(launch_lars<T>(a, shp.grid, shp.wpb, st));
         if (final_run) pr.launches(1);
@@ -845,7 +861,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
           a.work_counter = d_counter + 1; a.overflow_list = nullptr; a.overflow_count = nullptr;
           a.gstate = reinterpret_cast<T*>(W.gstate.ptr);
           a.rf_cap = refactor_cap(p.L);
-          if (p.chol) SC_CUDA(launch_lars_chol<T>(a, ov.grid, ov.wpb, st));
+          if (p.chol && shp.cta) SC_CUDA(launch_lars_chol_cta<T>(a, ov.grid, st));
+          else if (p.chol) SC_CUDA(launch_lars_chol<T>(a, ov.grid, ov.wpb, st));
           else if (shp.cta) SC_CUDA(launch_lars_cta<T>(a, ov.grid, st));
           else SC_CUDA(launch_lars<T>(a, ov.grid, ov.wpb, st));
         }
@@ -1250,11 +1267,8 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
     return fail(SC_ERR_UNSUPPORTED, "lasso : mode %d not supported by the coding path", mode);
   L = lasso_clamp<T>(m, K, L, lambda1, lambda2, mode, pos, &max_length_path);
   // ols or cholesky select the Cholesky implementation (lasso<T> / coreLARS,
-  // decomp/decomp.h:735-1093; _lassoD sets cholesky when ols is set), one
-  // warp per signal: dictionaries up to 1024 atoms
+  // decomp/decomp.h:735-1093; _lassoD sets cholesky when ols is set)
   const bool chol = ols || cholesky;
-  if (chol && K > 1024)
-    return fail(SC_ERR_UNSUPPORTED, "lasso : the Cholesky variant supports up to 1024 atoms (K = %d)", K);
   if (path) memset(path, 0, sizeof(T) * (size_t)K * std::max(0, max_length_path));
   if (L <= 0) return emit_empty<T>(0, 0, out);
   if (n == 0) return emit_empty<T>(K, 0, out);

@@ -141,6 +141,13 @@ int lars_cta_grid(int Kp, int Lc, bool gstate);
 template <typename T>
 cudaError_t launch_lars_chol(const LarsArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);
 size_t lars_chol_state_bytes(int Kp, int Lc, size_t esz);
+// Its CTA form: one CTA of Kp / 512 warps per signal (Kp as for
+// launch_lars_cta); a.gstate set: per-CTA small state in global slabs of
+// lars_chol_cta_gstate_bytes(a.Lcap, sizeof(T)).
+template <typename T>
+cudaError_t launch_lars_chol_cta(const LarsArgs<T>& a, int grid, cudaStream_t st);
+size_t lars_chol_cta_smem_bytes(int Kp, int Lc, size_t esz, bool gstate);
+size_t lars_chol_cta_gstate_bytes(int Lc, size_t esz);
 
 template <typename T>
 cudaError_t launch_omp(const OmpArgs<T>& a, int grid, int warps_per_block, cudaStream_t st);

@@ -63,3 +63,28 @@ def test_warp_kernel_refuses_large_dictionaries():
         spams_b200.omp(X, D, L=4, kernel="warp")
     assert e.value.status == _lib.SC_ERR_UNSUPPORTED
     _same(spams_b200.omp(X, D, L=4, kernel="cta"), spams_b200.omp(X, D, L=4))
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("m,K", [(64, 200), (128, 1000)])
+def test_cholesky_variant_warp_and_cta_give_the_same_bits(dt, m, K):
+    """The Cholesky implementation (cholesky / ols) in its two forms: the
+    warp kernel and, forced here at a size the warp kernel takes, the CTA
+    kernel that codes dictionaries beyond 1024 atoms."""
+    X, D = _draw(m, K, 300, K + m + 1, dt)
+    runs = [
+        dict(lambda1=0.05, cholesky=True),
+        dict(lambda1=0.005, cholesky=True),                 # past the 32-atom state
+        dict(lambda1=2.0, mode=0, pos=True, cholesky=True),
+        dict(lambda1=0.5, mode=1, cholesky=True),
+        dict(lambda1=0.05, ols=True),
+        dict(lambda1=0.5, mode=1, ols=True),
+    ]
+    for kw in runs:
+        w = spams_b200.lasso(X, D, kernel="warp", **kw)
+        c = spams_b200.lasso(X, D, kernel="cta", **kw)
+        _same(w, c)
+    pw = spams_b200.lasso(X, D, lambda1=0.02, cholesky=True, return_reg_path=True, kernel="warp")
+    pc = spams_b200.lasso(X, D, lambda1=0.02, cholesky=True, return_reg_path=True, kernel="cta")
+    _same(pw[0], pc[0])
+    np.testing.assert_array_equal(pw[1], pc[1])

@@ -56,6 +56,41 @@ def test_beyond_4096_atoms_exact_support_f64(K):
     assert support_match(a32, ref) >= 0.95
 
 
+@pytest.mark.parametrize("K", [1536, 4097])
+@pytest.mark.parametrize("variant", ["cholesky", "ols"])
+def test_cholesky_variant_beyond_1024_atoms_f64(K, variant):
+    """The Cholesky implementation (coreLARS + downDateLasso) on the CTA
+    kernel: every constraint mode, pos, and the active sets past the
+    shared-memory capacity (about 61 atoms at lambda 0.1 here)."""
+    X, D = _draw(64, K, 40, K + 5)
+    for mode, lam in [(2, 0.1), (0, 1.5), (1, 20.0)]:
+        for pos in (False, True):
+            ref = O.orc_lasso(X, D, lambda1=lam, mode=mode, pos=pos, **{variant: True})
+            a = spams_b200.lasso(X, D, lambda1=lam, mode=mode, pos=pos, **{variant: True})
+            assert a.shape == ref.shape
+            assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9, (mode, pos)
+
+
+def test_cholesky_variant_large_active_sets_and_path():
+    """120-atom active sets (the rerun with the state in global memory), the
+    path of signal 0, and the largest dictionary."""
+    X, D = _draw(160, 2048, 8, 77)
+    for variant in ("cholesky", "ols"):
+        ref, rpath = O.orc_lasso(X, D, L=120, lambda1=0.01, return_reg_path=True,
+                                 **{variant: True})
+        a, path = spams_b200.lasso(X, D, L=120, lambda1=0.01, return_reg_path=True,
+                                   **{variant: True})
+        assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+        np.testing.assert_allclose(path, rpath, rtol=1e-8, atol=1e-10)
+    X, D = _draw(48, 16384, 8, 16384)
+    ref = O.orc_lasso(X, D, lambda1=0.1, cholesky=True)
+    a = spams_b200.lasso(X, D, lambda1=0.1, cholesky=True)
+    assert support_match(a, ref) == 1.0 and rel_err(a, ref) <= 1e-9
+    a32 = spams_b200.lasso(X.astype(np.float32), D.astype(np.float32), lambda1=0.1,
+                           cholesky=True)
+    assert support_match(a32, ref) >= 0.95
+
+
 def test_more_than_16384_atoms_refused():
     X, D = _draw(16, 16385, 2, 3)
     with pytest.raises(spams_b200.ScError, match="16384"):
