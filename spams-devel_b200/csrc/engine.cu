@@ -1042,7 +1042,12 @@ struct CallGuard {
     if (!capturing) cudaStreamWaitEvent(st, c->last_use, 0);
   }
   ~CallGuard() {
-    if (!capturing) cudaEventRecord(c->last_use, st);
+    if (!capturing) {
+      cudaEventRecord(c->last_use, st);
+      // no copy-in of a caller's host buffer outlives the call, whatever its
+      // exit (on success every copy has long been consumed)
+      if (c->h2d_stream) cudaStreamSynchronize(c->h2d_stream);
+    }
   }
 };
 
@@ -1222,7 +1227,8 @@ static sc_status omp_host(const T* X, int m, int64_t n, const T* D, int K, const
   if (mask) {  // omp_mask: masked Grams get a 1e-10 ridge, eps scales (decomp/decomp.h:477-481)
     p.hmask = mask;
     p.mask_ridge = T(1e-10);
-    p.kernel = SC_KERNEL_WARP;
+    // the warp kernel unless a family is asked for (beyond 1024 atoms the CTA kernel)
+    if (p.kernel == SC_KERNEL_AUTO) p.kernel = SC_KERNEL_WARP;
     p.refine = false;
   }
   SC_TRY(run_pipeline<T>(*c, st, p, (const T*)c->G.ptr, &sink, d_capflag, pr));
@@ -1337,7 +1343,8 @@ static sc_status lasso_host(const T* X, int m, int64_t n, const T* D, const T* Q
     p.mask_ridge = lambda2 > T(1e-10) ? lambda2 : T(1e-10);
     p.mask_scale = (mode == SC_PENALTY || mode == SC_L2ERROR) ? 1 : 0;
     p.length_path = 4 * L;
-    p.kernel = SC_KERNEL_WARP;
+    // the warp kernel unless a family is asked for (beyond 1024 atoms the CTA kernel)
+    if (p.kernel == SC_KERNEL_AUTO) p.kernel = SC_KERNEL_WARP;
     p.refine = false;
     p.ols = false;
   }

@@ -110,12 +110,16 @@ def test_masked_on_the_cta_kernels_f64(m, K):
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 def test_masked_warp_and_cta_kernels_give_the_same_bits(dt):
+    """Masked coding on the warp kernel (the default up to 1024 atoms) and
+    on the CTA kernel when asked for."""
     X, D, B = _draw(48, 512, 300, 17)
     Xd, Dd = X.astype(dt), D.astype(dt)
-    _same(spams_b200.ompMask(Xd, Dd, B, L=10, kernel="warp"),
-          spams_b200.ompMask(Xd, Dd, B, L=10, kernel="cta"))
-    _same(spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="warp"),
-          spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="cta"))
+    w = spams_b200.ompMask(Xd, Dd, B, L=10, kernel="warp")
+    _same(w, spams_b200.ompMask(Xd, Dd, B, L=10))
+    _same(w, spams_b200.ompMask(Xd, Dd, B, L=10, kernel="cta"))
+    w = spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="warp")
+    _same(w, spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05))
+    _same(w, spams_b200.lassoMask(Xd, Dd, B, lambda1=0.05, kernel="cta"))
 
 
 def test_masked_limits():
