@@ -42,12 +42,40 @@ const char* last_error() { return g_err; }
 
 // ---------------------------------------------------------------------------
 // device buffers (grow-only, cached per device)
+static thread_local cudaStream_t t_alloc_stream = nullptr;
+AllocStream::AllocStream(cudaStream_t st) : prev(t_alloc_stream) { t_alloc_stream = st; }
+AllocStream::~AllocStream() { t_alloc_stream = prev; }
+
 sc_status Buf::reserve(size_t b) {
   if (b <= bytes) return SC_OK;
+  const size_t want = std::max(b, (size_t)256);
+  const cudaStream_t st = t_alloc_stream;
+  if (st) {
+    // stream-ordered: the old block goes back to the pool after the work
+    // already on `st`, the new one comes from the pool (no device-wide sync)
+    if (ptr) {
+      if (pooled) cudaFreeAsync(ptr, st);
+      else cudaFree(ptr);
+    }
+    ptr = nullptr;
+    bytes = 0;
+    pooled = false;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, want, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // usable on every stream
+    if (e == cudaSuccess) {
+      ptr = p;
+      bytes = want;
+      pooled = true;
+      return SC_OK;
+    }
+    if (p) cudaFreeAsync(p, st);
+    cudaGetLastError();  // fall back to cudaMalloc below
+  }
   if (ptr) cudaFree(ptr);
   ptr = nullptr;
   bytes = 0;
-  const size_t want = std::max(b, (size_t)256);
+  pooled = false;
   cudaError_t e = cudaMalloc(&ptr, want);
   if (e != cudaSuccess) {
     ptr = nullptr;
@@ -59,9 +87,10 @@ sc_status Buf::reserve(size_t b) {
   return SC_OK;
 }
 void Buf::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) cudaFree(ptr);  // (also for stream-ordered blocks: synchronises)
   ptr = nullptr;
   bytes = 0;
+  pooled = false;
 }
 
 sc_status DeviceCtx::pinned_cols(size_t bytes) {
@@ -108,6 +137,14 @@ sc_status create_ctx(int device, DeviceCtx** out) {
     SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
     SC_CUDA(cudaDeviceGetAttribute(&c->smem_per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     SC_CUDA(cudaHostAlloc(&c->pinned_small, 4096, cudaHostAllocDefault));
+    // the stream-ordered allocator keeps freed workspace blocks for reuse
+    // rather than unmapping them at every synchronisation (AllocStream)
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     SC_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
     SC_CUDA(cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking));
     SC_CUDA(cudaStreamCreateWithFlags(&c->lane[1].stream, cudaStreamNonBlocking));
@@ -286,7 +323,8 @@ struct TuneKey {
   }
 };
 static std::mutex g_tune_mu;
-static std::map<TuneKey, int> g_tune;  // key -> index into shape_candidates
+static std::map<TuneKey, int> g_tune;  // key -> index into shape_candidates, or kTuning
+constexpr int kTuning = -1;            // a call is timing the key's candidates
 
 static bool autotune_enabled() {
   static const bool on = [] {
@@ -689,23 +727,38 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
   int chosen = cands.size() == 1 ? 0 : -1;
   TuneKey key{p.lars ? 1 : 0, sizeof(T) == 8 ? 1 : 0, Kp, tune_lclass(p.L), 0, p.kernel,
               p.hmask ? 1 : 0};
-  {
-    int64_t c0 = std::min<int64_t>(nc, p.n), cls = 0;
-    while (c0 > 1) { c0 >>= 1; ++cls; }
-    key.nclass = (int)cls;
-  }
+  key.nclass = tune_nclass(std::min<int64_t>(nc, p.n));
   if (chosen < 0 && !autotune_enabled()) chosen = 0;
+  bool claimed = false;  // this call times the candidates for `key`
   if (chosen < 0) {
+    // one call per key times the candidates (kTuning marks the claim);
+    // calls that meet a claim meanwhile (other threads, serving slots) take
+    // the static rule's shape rather than time candidates concurrently
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
-    if (it != g_tune.end() && it->second < (int)cands.size()) chosen = it->second;
+    if (it == g_tune.end()) {
+      g_tune[key] = kTuning;
+      claimed = true;
+    } else {
+      chosen = it->second >= 0 && it->second < (int)cands.size() ? it->second : 0;
+    }
   }
+  struct TuneClaim {  // an unfinished claim is withdrawn, whatever the exit
+    bool& on;
+    TuneKey k;
+    ~TuneClaim() {
+      if (!on) return;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(k);
+      if (it != g_tune.end() && it->second == kTuning) g_tune.erase(it);
+    }
+  } tune_claim{claimed, key};
   auto tune = [&](int64_t cn, auto& code, int& out) -> sc_status {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     SC_CUDA(cudaStreamIsCapturing(st, &cap));
     if (cap != cudaStreamCaptureStatusNone) {  // no timing inside a graph capture
       out = 0;
-      return SC_OK;
+      return SC_OK;  // (the claim is withdrawn: a later call times the key)
     }
     const int64_t sample = std::min<int64_t>(cn, 16384);
     cudaEvent_t e0, e1;
@@ -736,6 +789,7 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
     out = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
+    claimed = false;
     return SC_OK;
   };
 
@@ -898,7 +952,8 @@ static sc_status run_pipeline(DeviceCtx& c, cudaStream_t st, Problem<T>& p, cons
       }
       return SC_OK;
     };
-    if (chosen < 0) SC_TRY(tune(cn, code, chosen));
+    if (chosen < 0 && claimed) SC_TRY(tune(cn, code, chosen));
+    if (chosen < 0) chosen = 0;
     const Shape& shp = cands[(size_t)chosen];
     const bool may_overflow = shp.Lcap < p.L;
     g_prof.kernel = shp.cta ? SC_KERNEL_CTA : SC_KERNEL_WARP;
@@ -1036,10 +1091,16 @@ struct CallGuard {
   cudaStream_t st;
   std::lock_guard<std::mutex> lk;
   bool capturing = false;
-  CallGuard(DeviceCtx* ctx, cudaStream_t s) : c(ctx), st(s), lk(ctx->mu) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    capturing = cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+  // workspace growth ordered on the call's stream after the previous call
+  // (none while capturing: growth there fails as before)
+  AllocStream alloc;
+  CallGuard(DeviceCtx* ctx, cudaStream_t s)
+      : c(ctx), st(s), lk(ctx->mu), capturing(is_capturing(s)), alloc(capturing ? nullptr : s) {
     if (!capturing) cudaStreamWaitEvent(st, c->last_use, 0);
+  }
+  static bool is_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
   }
   ~CallGuard() {
     if (!capturing) {

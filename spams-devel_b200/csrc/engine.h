@@ -35,8 +35,23 @@ const char* last_error();
 struct Buf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  bool pooled = false;  // from the stream-ordered allocator
   sc_status reserve(size_t b);
   void release();
+};
+
+// While one is in scope on a thread, Buf::reserve grows workspaces through
+// the stream-ordered allocator on `st` (the old block freed, the new one
+// allocated, then `st` alone waited for) instead of cudaFree / cudaMalloc,
+// whose implicit device-wide synchronisation stalls every other stream, other
+// serving slots' launches included, at each growth.  The scope's owner
+// guarantees that every earlier use of the thread's workspaces is ordered
+// before `st`'s current work (a call's guard after its wait on the previous
+// call; a serving slot after its previous batch completed).
+struct AllocStream {
+  cudaStream_t prev;
+  explicit AllocStream(cudaStream_t st);
+  ~AllocStream();
 };
 
 // Per-chunk workspaces of a coding lane.  Host-array calls code consecutive

@@ -147,6 +147,10 @@ sc_status run_batch(sc_server* s, Slot& sl, SrvDict& d, std::vector<SrvReq*>& ba
   DeviceCtx& c = *sl.ctx;
   cudaStream_t st = c.stream;
   SC_CUDA(cudaSetDevice(s->device));
+  // the slot's workspaces grow on its own stream (its previous batch has
+  // completed), not through a device-wide synchronisation that would stall
+  // the other slots
+  AllocStream grow_on(st);
   const SrvReq& r0 = *batch.front();
   const bool lars = r0.r.algo == SC_REQ_LASSO;
   int64_t N = 0;

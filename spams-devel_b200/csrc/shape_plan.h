@@ -113,6 +113,13 @@ inline std::vector<Shape> shape_candidates(const DeviceLimits& d, int Kp, int L,
 // different L.
 inline int tune_lclass(int L) { return L <= 32 ? 0 : (L <= 64 ? 1 : 2); }
 
+// ... and by the batch size (signals of the first chunk) through this class:
+// latency-bound batches (a few persistent waves at most), mid-size and large
+// ones.  A class per power of two made a serving stream, whose merged batches
+// span 1 to ~10^5 signals, tune the same dictionary again for every size,
+// each time on samples of up to 16384 signals per candidate.
+inline int tune_nclass(int64_t n) { return n < 512 ? 0 : (n < 4096 ? 1 : (n < 32768 ? 2 : 3)); }
+
 // A candidate replaces the one kept so far only below this fraction of its
 // sample time.
 constexpr float kTuneMargin = 0.95f;

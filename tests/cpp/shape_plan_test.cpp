@@ -103,6 +103,9 @@ int main() {
   // the tuner's key classes and its margin rule
   CHECK(tune_lclass(1) == 0 && tune_lclass(32) == 0 && tune_lclass(33) == 1);
   CHECK(tune_lclass(64) == 1 && tune_lclass(65) == 2 && tune_lclass(512) == 2);
+  CHECK(tune_nclass(1) == 0 && tune_nclass(511) == 0 && tune_nclass(512) == 1);
+  CHECK(tune_nclass(4095) == 1 && tune_nclass(4096) == 2 && tune_nclass(32767) == 2);
+  CHECK(tune_nclass(32768) == 3 && tune_nclass((int64_t)1 << 40) == 3);
   CHECK(pick_fastest({}) == 0);
   CHECK(pick_fastest({1.0f}) == 0);
   CHECK(pick_fastest({1.0f, 0.97f}) == 0);  // within the margin: the static rule's shape stays
