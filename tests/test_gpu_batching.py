@@ -67,3 +67,42 @@ def test_graph_replay_of_uneven_omp_matches_eager_call(prec):
         a = eager[:, :ns]
         assert support_match(a, ref) >= 0.995
         assert rel_err(*matched_columns(a, ref)) <= 1e-4
+
+
+def test_workspace_growth_between_calls_keeps_the_codes():
+    """Workspaces grow through the stream-ordered allocator on the call's
+    stream: a small call, a much larger one (every workspace grows), then the
+    small one again, on host arrays and on a caller's torch stream, give the
+    codes that each gives in isolation."""
+    rng = np.random.Generator(np.random.PCG64(41))
+    m, K = 96, 700
+    D = W.gaussian_dictionary(m, K, rng).astype(np.float32)
+    Xs, _, _ = W.sparse_signals(D, 300, 8, 0.01, rng)
+    Xb, _, _ = W.sparse_signals(D, 60000, 8, 0.01, rng)
+    Xs, Xb = np.asfortranarray(Xs, np.float32), np.asfortranarray(Xb, np.float32)
+    for prec in (spams_b200.SC_PREC_FP32, spams_b200.SC_PREC_BF16X3):
+        a1 = spams_b200.lasso(Xs, D, lambda1=0.05, precision=prec)
+        b1 = spams_b200.lasso(Xb, D, lambda1=0.05, precision=prec)
+        a2 = spams_b200.lasso(Xs, D, lambda1=0.05, precision=prec)
+        assert (a1 != a2).nnz == 0
+        b2 = spams_b200.lasso(Xb[:, :300], D, lambda1=0.05, precision=prec)
+        assert (b1[:, :300] != b2).nnz == 0
+        o1 = spams_b200.omp(Xs, D, L=10, precision=prec)
+        ob = spams_b200.omp(Xb, D, L=12, precision=prec)
+        assert (o1 != spams_b200.omp(Xs, D, L=10, precision=prec)).nnz == 0
+        assert (ob[:, -300:] != spams_b200.omp(Xb[:, -300:], D, L=12, precision=prec)).nnz == 0
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream()
+    def cm(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).to(dev).t()
+    Dd = cm(D)
+    with torch.cuda.stream(st):
+        small = spams_b200.lasso_device(cm(Xs), Dd, 0.05)
+        big = spams_b200.lasso_device(cm(Xb), Dd, 0.05)
+        again = spams_b200.lasso_device(cm(Xs), Dd, 0.05)
+    st.synchronize()
+    s1 = _csc(*small[:3], K, 300)
+    s2 = _csc(*again[:3], K, 300)
+    assert (s1 != s2).nnz == 0
+    assert (s1 != spams_b200.lasso(Xs, D, lambda1=0.05)).nnz == 0
+    assert _csc(*big[:3], K, 60000).nnz > 0
