@@ -332,7 +332,11 @@ sc_status sc_server_create(int device, int64_t hbm_budget_bytes, int slots,
                            int64_t max_batch_signals, sc_server** out);
 /* Codes the requests still pending, then frees everything. */
 sc_status sc_server_destroy(sc_server* s);
-/* Uploads D (host, m x K column-major) and forms its Grams (blocking). */
+/* Uploads D (host, m x K column-major) and forms its Grams (blocking).  Also
+ * grows the device's stream-ordered memory pool, from which the slots'
+ * workspaces are drawn, to slots x the workspace of a max_batch_signals batch
+ * on the largest dictionary added so far (within the budget), so that no
+ * slot grows the pool while requests run. */
 sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const float* D, int m,
                                        int K);
 /* Fails while requests against the dictionary are pending or in flight. */

@@ -99,6 +99,7 @@ struct sc_server {
   std::condition_variable cv_done;  // waiters: a request completed
   std::map<int64_t, std::unique_ptr<SrvDict>> dicts;
   size_t dict_bytes = 0;
+  size_t pool_warm = 0;  // bytes the stream-ordered pool was grown by for the slots
   std::deque<SrvReq*> pending;
   std::unordered_map<int64_t, SrvReq*> live;  // ticket -> request (until collected)
   std::vector<std::unique_ptr<Slot>> slots;
@@ -352,7 +353,12 @@ void slot_loop(sc_server* s, size_t idx) {
       if (s->active++ == 0) s->busy_from = Clock::now();
     }
     sc_status st = SC_OK;
-    if (!sl.ctx) st = create_ctx(s->device, &sl.ctx);
+    // a slot's page-locked parameter / column-pointer buffer, sized once for
+    // the largest batch (growing it frees page-locked memory, which waits for
+    // the whole device)
+    if (!sl.pinned) st = sl.host_buffer(3 * align16((size_t)s->max_batch * 4) +
+                                        (size_t)(s->max_batch + 1) * 8);
+    if (st == SC_OK && !sl.ctx) st = create_ctx(s->device, &sl.ctx);
     if (st == SC_OK) st = run_batch(s, sl, *d, batch);
     const std::string err = st == SC_OK ? std::string() : std::string(last_error());
     {
@@ -541,11 +547,36 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
     if (herr) return fail(SC_ERR_TIMEOUT, "serving: a bounded tensor-core pipeline wait gave up");
   }
   SC_CUDA(cudaStreamSynchronize(st));
+  size_t warm = 0;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->dict_bytes += d->bytes;
     s->peak = std::max(s->peak, s->reserved_total());
     s->dicts[dict_id] = std::move(d);
+    // the slots' workspaces come from the stream-ordered pool (AllocStream):
+    // grow it now, before any request, to what every slot needs for the
+    // largest batch on the largest dictionary, within the budget (growing
+    // the pool by gigabytes mid-stream stalled every slot for up to a second)
+    size_t need = 0;
+    for (auto& kv : s->dicts) {
+      const SrvDict& e = *kv.second;
+      need = std::max(need, batch_bytes(e.m, e.Kp, e.mp, std::min(e.m, e.K), s->max_batch, tcd) +
+                                ((size_t)256 << 20));
+    }
+    const size_t room = s->budget > s->dict_bytes ? s->budget - s->dict_bytes : 0;
+    const size_t target = std::min(need * s->slots.size(), room);
+    if (target > s->pool_warm) {
+      warm = target - s->pool_warm;
+      s->pool_warm = target;
+    }
+  }
+  if (warm > 0) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, warm, st) == cudaSuccess) {
+      cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+    }
+    cudaGetLastError();  // an unwarmed pool only costs time later
   }
   return SC_OK;
 }
