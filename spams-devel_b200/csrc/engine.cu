@@ -43,6 +43,14 @@ const char* last_error() { return g_err; }
 // ---------------------------------------------------------------------------
 // device buffers (grow-only, cached per device)
 static thread_local cudaStream_t t_alloc_stream = nullptr;
+
+// Gives the stream-ordered pool's free blocks of `device` back to the system
+// (after its streams' work: the caller has synchronised).
+void trim_pool(int device) {
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
+}
 AllocStream::AllocStream(cudaStream_t st) : prev(t_alloc_stream) { t_alloc_stream = st; }
 AllocStream::~AllocStream() { t_alloc_stream = prev; }
 
@@ -62,6 +70,15 @@ sc_status Buf::reserve(size_t b) {
     pooled = false;
     void* p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, want, st);
+    if (e == cudaErrorMemoryAllocation) {
+      // the pool's free blocks may be what is missing: return them, retry once
+      cudaGetLastError();
+      int dev = 0;
+      cudaStreamSynchronize(st);
+      if (cudaGetDevice(&dev) == cudaSuccess) trim_pool(dev);
+      p = nullptr;
+      e = cudaMallocAsync(&p, want, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // usable on every stream
     if (e == cudaSuccess) {
       ptr = p;
@@ -201,9 +218,11 @@ sc_status get_ctx(int device, DeviceCtx** out) {
 
 void release_all() {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
-  for (DeviceCtx*& c : g_ctx) {
-    destroy_ctx(c);
-    c = nullptr;
+  for (size_t dev = 0; dev < g_ctx.size(); ++dev) {
+    if (!g_ctx[dev]) continue;
+    destroy_ctx(g_ctx[dev]);
+    g_ctx[dev] = nullptr;
+    trim_pool((int)dev);
   }
 }
 

@@ -53,6 +53,9 @@ struct AllocStream {
   explicit AllocStream(cudaStream_t st);
   ~AllocStream();
 };
+// Returns the stream-ordered pool's free blocks of `device` to the system
+// (the pool otherwise keeps them for reuse): sc_release_all, server teardown.
+void trim_pool(int device);
 
 // Per-chunk workspaces of a coding lane.  Host-array calls code consecutive
 // chunks on two lanes (lane 1 on its own stream), so that one chunk's

@@ -490,6 +490,7 @@ sc_status sc_server_destroy(sc_server* s) {
                    &kv.second->GompTc, &kv.second->GlassoTc, &kv.second->tcerr})
       b->release();
   destroy_ctx(s->admin);
+  trim_pool(s->device);  // the slots' pool blocks (grown by add_dictionary) go back
   delete s;
   return SC_OK;
 }
