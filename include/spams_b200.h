@@ -126,7 +126,9 @@ const char* sc_last_error(void);          /* thread-local message of the last fa
 sc_status sc_device_count(int* count);    /* number of usable CUDA devices */
 void sc_csc_free_f32(sc_csc_f32* a);      /* frees colptr/rows/vals, zeroes the struct */
 void sc_csc_free_f64(sc_csc_f64* a);
-/* Releases the engine's cached device workspaces and streams on all devices. */
+/* Releases the engine's cached device workspaces and streams on all devices,
+ * returns the free blocks of the stream-ordered memory pool the workspaces
+ * grow from to the device, and frees the unused page-locked result blocks. */
 void sc_release_all(void);
 /* Copies the calling thread's last-call profile (see sc_profile). */
 sc_status sc_last_profile(sc_profile* out);
