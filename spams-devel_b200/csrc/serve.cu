@@ -564,8 +564,7 @@ sc_status sc_server_add_dictionary_f32(sc_server* s, int64_t dict_id, const floa
       need = std::max(need, batch_bytes(e.m, e.Kp, e.mp, std::min(e.m, e.K), s->max_batch, tcd) +
                                 ((size_t)256 << 20));
     }
-    const size_t room = s->budget > s->dict_bytes ? s->budget - s->dict_bytes : 0;
-    const size_t target = std::min(need * s->slots.size(), room);
+    const size_t target = pool_target(need, s->slots.size(), s->budget, s->dict_bytes);
     if (target > s->pool_warm) {
       warm = target - s->pool_warm;
       s->pool_warm = target;

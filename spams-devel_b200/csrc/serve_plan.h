@@ -63,6 +63,14 @@ inline size_t batch_bytes(int m, int Kp, int mp, int L, int64_t n, bool tc) {
   return per * (size_t)std::max<int64_t>(n, 1) + ((size_t)1 << 20);
 }
 
+// What the stream-ordered pool should hold for the slots, given the largest
+// batch workspace over the resident dictionaries (`need`): every slot's
+// largest batch, within what the budget leaves after the dictionaries.
+inline size_t pool_target(size_t need, size_t slots, size_t budget, size_t dict_bytes) {
+  const size_t room = budget > dict_bytes ? budget - dict_bytes : 0;
+  return std::min(need * slots, room);
+}
+
 // Admission: the resident dictionaries plus what every slot holds must stay
 // within the budget.  A slot's workspaces only grow, so slot s holding
 // `reserved[s]` bytes and needing `need` ends up holding the larger of both.

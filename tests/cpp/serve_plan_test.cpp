@@ -89,6 +89,10 @@ int main() {
     CHECK(percentile({7}, 99) == 7);
   }
   if (failures) return 1;
+  // the pool warm-up: every slot's largest batch, within the budget's room
+  CHECK(pool_target(100, 3, 1000, 200) == 300);
+  CHECK(pool_target(400, 3, 1000, 200) == 800);
+  CHECK(pool_target(400, 3, 100, 200) == 0);
   std::printf("serve_plan: all checks passed\n");
   return 0;
 }
